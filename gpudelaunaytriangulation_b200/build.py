@@ -1,0 +1,79 @@
+"""In-tree build of the CUDA library: gpudelaunaytriangulation_b200/_lib/libdgt.so (sm_100a).
+
+nvcc cross-compiles without a GPU, so this runs in the build container and the .so travels
+with the source tree.  Re-run when a source under csrc/ or include/ changes.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+INCLUDE = os.path.join(ROOT, "include")
+LIBDIR = os.path.join(PKG, "_lib")
+LIB = os.path.join(LIBDIR, "libdgt.so")
+SOURCES = ["dgt_bin.cu", "dgt_ring.cu", "dgt_api.cu"]
+HEADERS = ["dgt_internal.cuh", "dgt_predicates.cuh"]
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _inputs():
+    files = [os.path.join(CSRC, s) for s in SOURCES + HEADERS] + [os.path.join(INCLUDE, "dgt.h")]
+    return files
+
+
+def stale() -> bool:
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    return any(os.path.getmtime(f) > t for f in _inputs())
+
+
+def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None) -> str:
+    if not force and not stale():
+        return LIB
+    os.makedirs(os.path.join(LIBDIR, "obj"), exist_ok=True)
+    objs = []
+    procs = []
+    for src in SOURCES:
+        obj = os.path.join(LIBDIR, "obj", src.replace(".cu", ".o"))
+        cmd = [nvcc(), *NVFLAGS, *ARCH, "-I", INCLUDE, "-I", CSRC, "-c", os.path.join(CSRC, src), "-o", obj]
+        if extra:
+            cmd[1:1] = extra
+        if verbose:
+            print(" ".join(cmd))
+        procs.append((subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT), src))
+        objs.append(obj)
+    errors = []
+    for p, src in procs:
+        out, _ = p.communicate()
+        if p.returncode != 0:
+            errors.append(f"{src}:\n{out.decode(errors='replace')}")
+        elif verbose and out:
+            print(out.decode(errors="replace"))
+    if errors:
+        raise RuntimeError("nvcc failed:\n" + "\n".join(errors))
+    tmp = LIB + ".tmp"
+    cmd = [nvcc(), "-shared", *ARCH, "-o", tmp, *objs, "-lcudart"]
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True,
+          extra=["-Xptxas", "-v"] if "--ptxas" in sys.argv else None)
+    print(LIB)

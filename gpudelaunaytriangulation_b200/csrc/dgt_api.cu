@@ -1,0 +1,551 @@
+// C ABI of the library (include/dgt.h): context, scratch memory and the call sequences.
+//
+// global triangulation   bin -> build (all points, cell order) -> slow path (device list)
+// test and repair        bin -> local test (queue) -> rounds of rebuild over the queue
+//
+// Repair rounds.  The test queues every point whose fan is not certainly Delaunay, with
+// the vertices of each failing spoke's quadrilateral.  A round rebuilds its queued points
+// from scratch (exact rings) and queues, for the next round, every point not yet rebuilt in
+// this call whose ring the rebuilt ring contradicts: an old neighbour that was dropped, or a
+// new neighbour whose ring does not list the point with the same two adjacent neighbours.
+// At the fixed point every point is either rebuilt (exact) or untouched, untouched fans
+// passed the local test and agree with every neighbour, so all edges are locally Delaunay
+// in a consistent triangulation of the torus, which makes it the Delaunay triangulation
+// (Lawson).  Marks are epochs (mark[i] >= base: already queued in this call), so nothing is
+// cleared between calls and each point is rebuilt at most once per call.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "dgt.h"
+#include "dgt_internal.cuh"
+
+using namespace dgt;
+
+namespace {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t want)
+    {
+        if (p && bytes >= want) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, want ? want : 16);
+        if (e == cudaSuccess) bytes = want ? want : 16;
+        return e;
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <typename T> T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+constexpr int SLOW_ITEMS = 2048;    // concurrent exact / large-ring items (scratch rows)
+constexpr int ASYNC_ROUNDS = 8;     // repair rounds launched before the first host check
+
+}  // namespace
+
+struct dgt_context {
+    int device = 0;
+    int num_sets = 1;
+    int n = 0;
+    bool batch = false;
+    std::vector<int> sizes;
+    std::vector<double> boxes;
+    double cell_size = 1.0;
+    int max_size = 16;
+    int safety = 1;
+    int precision = DGT_PRECISION_FP32_FILTER;
+    int check = 0;
+    int deterministic = 1;
+    std::vector<SetDesc> sets;
+    int total_cells = 0;
+    int epoch = 0;
+    DevBuf d_sets, d_set_of, ccount, cstart, cell_of, rank, sidx, slot_of, spos, bsum, mark, list0, list1,
+        slow_list, slow_scratch, st;
+    DevStatus *h_st = nullptr;
+    cudaStream_t last_stream = nullptr;
+    bool stats_valid = false;
+    int pending_rounds_check = 0;   // repair launched without a host check (safety off)
+};
+
+namespace {
+
+int cuda_status(cudaError_t e)
+{
+    if (e == cudaSuccess) return DGT_OK;
+    if (e == cudaErrorMemoryAllocation) return DGT_ERR_OUT_OF_MEMORY;
+    return DGT_ERR_CUDA;
+}
+
+#define DGT_TRY(expr)                                   \
+    do {                                                \
+        cudaError_t e_ = (expr);                        \
+        if (e_ != cudaSuccess) return cuda_status(e_);  \
+    } while (0)
+
+double pow2_at_least(double x)
+{
+    double v = 1.0;
+    while (v < x) v *= 2.0;
+    return v;
+}
+
+// cell grid of every set from the requested cell edge
+int plan_grid(dgt_context *c)
+{
+    c->sets.assign(c->num_sets, SetDesc());
+    long long cells = 0;
+    int pbase = 0;
+    for (int s = 0; s < c->num_sets; ++s) {
+        double Lx = c->boxes[2 * s], Ly = c->boxes[2 * s + 1];
+        int ns = c->sizes[s];
+        double spacing = std::sqrt(Lx * Ly / std::max(ns, 1));
+        double a;
+        if (c->batch) a = (c->cell_size > 0 ? c->cell_size : 1.0) * spacing;
+        else a = c->cell_size > 0 ? c->cell_size : spacing;
+        // keep the grid within a few cells per point (tiny cells only cost memory and scans)
+        double amin = std::sqrt(Lx * Ly / (4.0 * std::max(ns, 1) + 16.0));
+        if (a < amin) a = amin;
+        int xs = std::max(1, (int)std::floor(Lx / a));
+        int ys = std::max(1, (int)std::floor(Ly / a));
+        SetDesc &S = c->sets[s];
+        S.Lx = Lx;
+        S.Ly = Ly;
+        S.hLx = 0.5 * Lx;
+        S.hLy = 0.5 * Ly;
+        S.xsize = xs;
+        S.ysize = ys;
+        S.cw = Lx / xs;
+        S.ch = Ly / ys;
+        S.icw = (double)xs / Lx;
+        S.ich = (double)ys / Ly;
+        S.cell_base = (int)cells;
+        S.point_base = pbase;
+        S.n = ns;
+        S.V = (float)pow2_at_least(std::max(Lx, Ly));
+        S.pad = 0;
+        cells += (long long)xs * ys;
+        pbase += ns;
+        if (cells > (1LL << 30)) return DGT_ERR_INVALID_ARGUMENT;
+    }
+    c->total_cells = (int)cells;
+    return DGT_OK;
+}
+
+int alloc_all(dgt_context *c)
+{
+    int n = std::max(c->n, 1);
+    size_t C = (size_t)c->total_cells + 1;
+    DGT_TRY(c->d_sets.ensure(sizeof(SetDesc) * c->sets.size()));
+    DGT_TRY(cudaMemcpy(c->d_sets.p, c->sets.data(), sizeof(SetDesc) * c->sets.size(), cudaMemcpyHostToDevice));
+    if (c->batch) {
+        std::vector<int> so(c->n);
+        for (int s = 0; s < c->num_sets; ++s)
+            for (int k = 0; k < c->sizes[s]; ++k) so[c->sets[s].point_base + k] = s;
+        DGT_TRY(c->d_set_of.ensure(sizeof(int) * n));
+        DGT_TRY(cudaMemcpy(c->d_set_of.p, so.data(), sizeof(int) * c->n, cudaMemcpyHostToDevice));
+    }
+    DGT_TRY(c->ccount.ensure(sizeof(int) * C));
+    DGT_TRY(c->cstart.ensure(sizeof(int) * C));
+    DGT_TRY(c->bsum.ensure(sizeof(int) * (scan_block_count((int)C) + 1)));
+    DGT_TRY(c->cell_of.ensure(sizeof(int) * n));
+    DGT_TRY(c->rank.ensure(sizeof(int) * n));
+    DGT_TRY(c->sidx.ensure(sizeof(int) * n));
+    DGT_TRY(c->slot_of.ensure(sizeof(int) * n));
+    DGT_TRY(c->spos.ensure(sizeof(double2) * n));
+    DGT_TRY(c->list0.ensure(sizeof(int) * n));
+    DGT_TRY(c->list1.ensure(sizeof(int) * n));
+    DGT_TRY(c->slow_list.ensure(sizeof(int) * n));
+    DGT_TRY(c->slow_scratch.ensure(slow_scratch_bytes_per_item(64) * SLOW_ITEMS));
+    bool fresh_mark = c->mark.bytes < sizeof(int) * (size_t)n;
+    DGT_TRY(c->mark.ensure(sizeof(int) * n));
+    if (fresh_mark) {
+        DGT_TRY(cudaMemset(c->mark.p, 0, sizeof(int) * n));
+        c->epoch = 0;
+    }
+    DGT_TRY(c->st.ensure(sizeof(DevStatus)));
+    if (!c->h_st) DGT_TRY(cudaMallocHost(&c->h_st, sizeof(DevStatus)));
+    return DGT_OK;
+}
+
+int init_context(dgt_context *c)
+{
+    int r = plan_grid(c);
+    if (r != DGT_OK) return r;
+    return alloc_all(c);
+}
+
+BinArgs bin_args(dgt_context *c, const double *pts)
+{
+    BinArgs a;
+    a.pos = reinterpret_cast<const double2 *>(pts);
+    a.n = c->n;
+    a.sets = c->d_sets.as<SetDesc>();
+    a.set_of = c->batch ? c->d_set_of.as<int>() : nullptr;
+    a.total_cells = c->total_cells;
+    a.ccount = c->ccount.as<int>();
+    a.cstart = c->cstart.as<int>();
+    a.cell_of = c->cell_of.as<int>();
+    a.rank = c->rank.as<int>();
+    a.sidx = c->sidx.as<int>();
+    a.slot_of = c->slot_of.as<int>();
+    a.spos = c->spos.as<double2>();
+    a.block_sums = c->bsum.as<int>();
+    a.deterministic = c->deterministic;
+    return a;
+}
+
+cudaError_t run_bin(dgt_context *c, const double *pts, cudaStream_t s)
+{
+    cudaError_t e = cudaMemsetAsync(c->ccount.p, 0, sizeof(int) * ((size_t)c->total_cells + 1), s);
+    if (e != cudaSuccess) return e;
+    return launch_bin_st(bin_args(c, pts), c->st.as<DevStatus>(), s);
+}
+
+RingArgs ring_args(dgt_context *c, const double *pts, int *tri, int *nn, int stride)
+{
+    RingArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.sets = c->d_sets.as<SetDesc>();
+    a.set_of = c->batch ? c->d_set_of.as<int>() : nullptr;
+    a.pos = reinterpret_cast<const double2 *>(pts);
+    a.spos = c->spos.as<double2>();
+    a.sidx = c->sidx.as<int>();
+    a.slot_of = c->slot_of.as<int>();
+    a.cstart = c->cstart.as<int>();
+    a.tri = tri;
+    a.nn = nn;
+    a.stride = stride;
+    a.npoints = c->n;
+    a.n_items = c->n;
+    a.mark = c->mark.as<int>();
+    a.slow_list = c->slow_list.as<int>();
+    a.slow_count = &c->st.as<DevStatus>()->slow_count;
+    a.check = c->check;
+    a.st = c->st.as<DevStatus>();
+    return a;
+}
+
+cudaError_t run_slow(dgt_context *c, const RingArgs &a, cudaStream_t s)
+{
+    return launch_slow(a, c->slow_scratch.p, SLOW_ITEMS, 64, s);
+}
+
+void to_stats(const DevStatus &d, dgt_stats *o)
+{
+    std::memset(o, 0, sizeof(*o));
+    o->points = (long long)d.points;
+    o->candidates = (long long)d.candidates;
+    o->tests = (long long)d.tests;
+    o->fp32_undecided = (long long)d.f32_undecided;
+    o->fp64_undecided = (long long)d.f64_undecided;
+    o->exact_points = (long long)d.exact_points;
+    o->mismatches = (long long)d.mismatches;
+    o->insertions = (long long)d.insertions;
+    o->flagged = (long long)d.flagged;
+    o->repaired = (long long)d.repaired;
+    o->repair_rounds = d.rounds;
+    o->max_ring = d.max_ring;
+    o->error_flags = d.err_flags;
+}
+
+// read the device status (synchronising) and turn it into a status code
+int conclude(dgt_context *c, cudaStream_t s, bool repair_pending)
+{
+    DGT_TRY(cudaMemcpyAsync(c->h_st, c->st.p, sizeof(DevStatus), cudaMemcpyDeviceToHost, s));
+    DGT_TRY(cudaStreamSynchronize(s));
+    c->stats_valid = true;
+    const DevStatus &d = *c->h_st;
+    if (d.err_flags & EF_BAD_INPUT) return DGT_ERR_BAD_POINTS;
+    if (d.need_stride > 0) {
+        c->max_size = std::max(c->max_size, d.need_stride);
+        return DGT_ERR_NEED_RESIZE;
+    }
+    if (d.err_flags) return DGT_ERR_DEGENERATE;
+    if (repair_pending) return DGT_ERR_NOT_CONVERGED;
+    return DGT_OK;
+}
+
+bool valid_stride(int stride) { return stride >= 3 && stride <= (1 << 16); }
+
+}  // namespace
+
+extern "C" {
+
+int dgt_version(void) { return 1; }
+
+const char *dgt_error_string(int code)
+{
+    switch (code) {
+    case DGT_OK: return "ok";
+    case DGT_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case DGT_ERR_CUDA: return "CUDA error";
+    case DGT_ERR_NEED_RESIZE: return "a ring is longer than the row stride (see dgt_get_max_size)";
+    case DGT_ERR_DEGENERATE: return "degenerate input: a ring could not be closed";
+    case DGT_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case DGT_ERR_BAD_POINTS: return "a coordinate lies outside [0, L) or is not finite";
+    case DGT_ERR_NOT_CONVERGED: return "repair did not reach a fixed point";
+    default: return "unknown error";
+    }
+}
+
+int dgt_create(int n, int max_neighs, double cell_size, double Lx, double Ly, dgt_context **out)
+{
+    if (!out) return DGT_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (n < 0 || !(Lx > 0) || !(Ly > 0) || !std::isfinite(Lx) || !std::isfinite(Ly) || !std::isfinite(cell_size))
+        return DGT_ERR_INVALID_ARGUMENT;
+    dgt_context *c = new (std::nothrow) dgt_context();
+    if (!c) return DGT_ERR_OUT_OF_MEMORY;
+    cudaGetDevice(&c->device);
+    c->n = n;
+    c->num_sets = 1;
+    c->sizes.assign(1, n);
+    c->boxes = { Lx, Ly };
+    c->cell_size = cell_size;
+    c->max_size = std::max(4, max_neighs);   // DelaunayGPU.cpp:21
+    int r = init_context(c);
+    if (r != DGT_OK) {
+        dgt_destroy(c);
+        return r;
+    }
+    *out = c;
+    return DGT_OK;
+}
+
+int dgt_create_batch(int num_sets, const int *sizes, const double *boxes, double cell_size, int max_neighs,
+                     dgt_context **out)
+{
+    if (!out) return DGT_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (num_sets <= 0 || !sizes || !boxes || !std::isfinite(cell_size)) return DGT_ERR_INVALID_ARGUMENT;
+    long long total = 0;
+    for (int s = 0; s < num_sets; ++s) {
+        if (sizes[s] < 0 || !(boxes[2 * s] > 0) || !(boxes[2 * s + 1] > 0) || !std::isfinite(boxes[2 * s]) ||
+            !std::isfinite(boxes[2 * s + 1]))
+            return DGT_ERR_INVALID_ARGUMENT;
+        total += sizes[s];
+    }
+    if (total > (1LL << 30)) return DGT_ERR_INVALID_ARGUMENT;
+    dgt_context *c = new (std::nothrow) dgt_context();
+    if (!c) return DGT_ERR_OUT_OF_MEMORY;
+    cudaGetDevice(&c->device);
+    c->batch = true;
+    c->num_sets = num_sets;
+    c->n = (int)total;
+    c->sizes.assign(sizes, sizes + num_sets);
+    c->boxes.assign(boxes, boxes + 2 * num_sets);
+    c->cell_size = cell_size;
+    c->max_size = std::max(4, max_neighs);
+    int r = init_context(c);
+    if (r != DGT_OK) {
+        dgt_destroy(c);
+        return r;
+    }
+    *out = c;
+    return DGT_OK;
+}
+
+void dgt_destroy(dgt_context *c)
+{
+    if (!c) return;
+    DevBuf *bufs[] = { &c->d_sets, &c->d_set_of, &c->ccount, &c->cstart, &c->cell_of, &c->rank, &c->sidx,
+                       &c->slot_of, &c->spos, &c->bsum, &c->mark, &c->list0, &c->list1, &c->slow_list,
+                       &c->slow_scratch, &c->st };
+    for (DevBuf *b : bufs) b->release();
+    if (c->h_st) cudaFreeHost(c->h_st);
+    delete c;
+}
+
+int dgt_update_list(dgt_context *c, const double *d_points, void *stream)
+{
+    if (!c || (c->n > 0 && !d_points)) return DGT_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = (cudaStream_t)stream;
+    DGT_TRY(cudaMemsetAsync(c->st.p, 0, sizeof(DevStatus), s));
+    DGT_TRY(run_bin(c, d_points, s));
+    c->last_stream = s;
+    return DGT_OK;
+}
+
+int dgt_global_triangulation(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, int stride,
+                             void *stream)
+{
+    if (!c) return DGT_ERR_INVALID_ARGUMENT;
+    if (c->n == 0) return DGT_OK;   // DelaunayGPU.cpp:121-125: nothing to do
+    if (!d_points || !d_tri || !d_nn || !valid_stride(stride)) return DGT_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = (cudaStream_t)stream;
+    c->last_stream = s;
+    c->stats_valid = false;
+    DGT_TRY(cudaMemsetAsync(c->st.p, 0, sizeof(DevStatus), s));
+    DGT_TRY(run_bin(c, d_points, s));
+    RingArgs a = ring_args(c, d_points, d_tri, d_nn, stride);
+    DGT_TRY(launch_build(a, c->precision == DGT_PRECISION_FP64 ? MODE_F64 : MODE_F32, s));
+    DGT_TRY(run_slow(c, a, s));
+    if (!c->safety) return DGT_OK;
+    return conclude(c, s, false);
+}
+
+int dgt_test_and_repair(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, int stride, void *stream)
+{
+    if (!c) return DGT_ERR_INVALID_ARGUMENT;
+    if (c->n == 0) return DGT_OK;
+    if (!d_points || !d_tri || !d_nn || !valid_stride(stride)) return DGT_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = (cudaStream_t)stream;
+    c->last_stream = s;
+    c->stats_valid = false;
+    DevStatus *dst = c->st.as<DevStatus>();
+    DGT_TRY(cudaMemsetAsync(c->st.p, 0, sizeof(DevStatus), s));
+    DGT_TRY(run_bin(c, d_points, s));
+    const int base = c->epoch + 1;
+    int *lists[2] = { c->list0.as<int>(), c->list1.as<int>() };
+    TestArgs t;
+    t.sets = c->d_sets.as<SetDesc>();
+    t.set_of = c->batch ? c->d_set_of.as<int>() : nullptr;
+    t.pos = reinterpret_cast<const double2 *>(d_points);
+    t.tri = d_tri;
+    t.nn = d_nn;
+    t.stride = stride;
+    t.n = c->n;
+    t.mark = c->mark.as<int>();
+    t.epoch_base = base;
+    t.list = lists[0];
+    t.list_count = &dst->list_count[0];
+    t.st = dst;
+    DGT_TRY(launch_test(t, s));
+    const int mode = c->precision == DGT_PRECISION_FP64 ? MODE_F64 : MODE_F32;
+    int round = 0;
+    bool pending = false;
+    for (;;) {
+        // launch a batch of rounds; each kernel reads its item count on the device
+        int batch = ASYNC_ROUNDS;
+        for (int b = 0; b < batch; ++b, ++round) {
+            int cur = round & 1, nxt = cur ^ 1;
+            DGT_TRY(cudaMemsetAsync(&dst->list_count[nxt], 0, sizeof(int), s));
+            DGT_TRY(cudaMemsetAsync(&dst->slow_count, 0, sizeof(int), s));
+            RingArgs a = ring_args(c, d_points, d_tri, d_nn, stride);
+            a.worklist = lists[cur];
+            a.worklist_count = &dst->list_count[cur];
+            a.n_items = c->n;
+            a.repair = 1;
+            a.epoch_base = base;
+            a.epoch = base + round;
+            a.next_list = lists[nxt];
+            a.next_count = &dst->list_count[nxt];
+            DGT_TRY(launch_build(a, mode, s));
+            DGT_TRY(run_slow(c, a, s));
+        }
+        if (!c->safety) {
+            c->epoch = base + round;
+            pending = false;
+            return DGT_OK;
+        }
+        int left = 0;
+        DGT_TRY(cudaMemcpyAsync(&left, &dst->list_count[round & 1], sizeof(int), cudaMemcpyDeviceToHost, s));
+        DGT_TRY(cudaStreamSynchronize(s));
+        if (left == 0) break;
+        if (round > 4 * ASYNC_ROUNDS + 64) {
+            pending = true;
+            break;
+        }
+    }
+    c->epoch = base + round;
+    return conclude(c, s, pending);
+}
+
+int dgt_set_cell_size(dgt_context *c, double cell_size)
+{
+    if (!c || !std::isfinite(cell_size)) return DGT_ERR_INVALID_ARGUMENT;
+    c->cell_size = cell_size;
+    return init_context(c);
+}
+
+int dgt_set_box(dgt_context *c, double Lx, double Ly)
+{
+    if (!c || c->batch || !(Lx > 0) || !(Ly > 0) || !std::isfinite(Lx) || !std::isfinite(Ly))
+        return DGT_ERR_INVALID_ARGUMENT;
+    c->boxes = { Lx, Ly };
+    return init_context(c);
+}
+
+int dgt_set_safety_mode(dgt_context *c, int on)
+{
+    if (!c) return DGT_ERR_INVALID_ARGUMENT;
+    c->safety = on ? 1 : 0;
+    return DGT_OK;
+}
+
+int dgt_set_precision(dgt_context *c, int precision)
+{
+    if (!c || (precision != DGT_PRECISION_FP32_FILTER && precision != DGT_PRECISION_FP64))
+        return DGT_ERR_INVALID_ARGUMENT;
+    c->precision = precision;
+    return DGT_OK;
+}
+
+int dgt_set_check_mode(dgt_context *c, int on)
+{
+    if (!c) return DGT_ERR_INVALID_ARGUMENT;
+    c->check = on ? 1 : 0;
+    return DGT_OK;
+}
+
+int dgt_resize(dgt_context *c, int max_neighs)
+{
+    if (!c || max_neighs < 3) return DGT_ERR_INVALID_ARGUMENT;
+    c->max_size = max_neighs;
+    return DGT_OK;
+}
+
+int dgt_get_max_size(const dgt_context *c, int *out)
+{
+    if (!c || !out) return DGT_ERR_INVALID_ARGUMENT;
+    *out = c->max_size;
+    return DGT_OK;
+}
+
+int dgt_get_num_points(const dgt_context *c, int *out)
+{
+    if (!c || !out) return DGT_ERR_INVALID_ARGUMENT;
+    *out = c->n;
+    return DGT_OK;
+}
+
+int dgt_restride(const int *d_src, int src_stride, int *d_dst, int dst_stride, const int *d_nn, int n, void *stream)
+{
+    if (n < 0 || (n > 0 && (!d_src || !d_dst)) || src_stride < 1 || dst_stride < 1 || d_src == d_dst)
+        return DGT_ERR_INVALID_ARGUMENT;
+    DGT_TRY(launch_restride(d_src, src_stride, d_dst, dst_stride, d_nn, n, (cudaStream_t)stream));
+    return DGT_OK;
+}
+
+int dgt_get_stats(dgt_context *c, dgt_stats *out)
+{
+    if (!c || !out) return DGT_ERR_INVALID_ARGUMENT;
+    if (!c->stats_valid) {
+        DGT_TRY(cudaMemcpyAsync(c->h_st, c->st.p, sizeof(DevStatus), cudaMemcpyDeviceToHost, c->last_stream));
+        DGT_TRY(cudaStreamSynchronize(c->last_stream));
+        c->stats_valid = true;
+    }
+    to_stats(*c->h_st, out);
+    return DGT_OK;
+}
+
+int dgt_displace(dgt_context *c, double *d_points, double sigma, unsigned long long seed, unsigned long long step,
+                 void *stream)
+{
+    if (!c || (c->n > 0 && !d_points) || !(sigma >= 0) || !std::isfinite(sigma)) return DGT_ERR_INVALID_ARGUMENT;
+    DGT_TRY(launch_displace(reinterpret_cast<double2 *>(d_points), c->n, c->d_sets.as<SetDesc>(),
+                            c->batch ? c->d_set_of.as<int>() : nullptr, sigma, seed, step, (cudaStream_t)stream));
+    return DGT_OK;
+}
+
+}  // extern "C"

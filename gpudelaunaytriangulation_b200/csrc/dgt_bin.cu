@@ -1,0 +1,226 @@
+// Bucket grid as a CSR counting sort by cell (replaces the reference's fixed-capacity
+// buckets idxs[bin*Nmax+k] with an overflow-retry loop, cellListGPU.cpp:404-460 and
+// cellListGPU.cu:20-58):
+//   count    cell of every point (floor(x / cell edge), clamped), atomic rank in its cell
+//   scan     exclusive prefix sum of the counts -> cstart (one pass of reduce / scan / apply)
+//   scatter  slot = cstart[cell] + rank; cell-order copies of index and position
+//   order    points of a cell sorted by index, so the cell order (and every candidate order
+//            derived from it) is independent of atomic arrival order
+// No host round trip: capacity is exact by construction.
+#include "dgt_internal.cuh"
+
+namespace dgt {
+
+__device__ __forceinline__ int cell_index(const SetDesc &S, double2 p)
+{
+    int cx = (int)floor(p.x * S.icw), cy = (int)floor(p.y * S.ich);
+    cx = min(max(cx, 0), S.xsize - 1);
+    cy = min(max(cy, 0), S.ysize - 1);
+    return S.cell_base + cy * S.xsize + cx;
+}
+
+__global__ void __launch_bounds__(256) k_count(BinArgs a, DevStatus *st)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const SetDesc &S = a.sets[a.set_of ? a.set_of[i] : 0];
+    double2 p = a.pos[i];
+    if (!(p.x >= 0.0 && p.x < S.Lx && p.y >= 0.0 && p.y < S.Ly)) {
+        atomicOr(&st->err_flags, EF_BAD_INPUT);
+        p = make_double2(0.0, 0.0);
+    }
+    int c = cell_index(S, p);
+    a.cell_of[i] = c;
+    a.rank[i] = atomicAdd(&a.ccount[c], 1);
+}
+
+constexpr int SCAN_THREADS = 1024;
+constexpr int SCAN_ITEMS = 4;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+// block-wide exclusive scan of per-thread values; returns the block total in *total
+__device__ __forceinline__ int block_exclusive(int v, int *wsum, int *total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        int w = lane < (blockDim.x >> 5) ? wsum[lane] : 0;
+        int wi = w;
+        for (int o = 1; o < 32; o <<= 1) {
+            int t = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += t;
+        }
+        wsum[lane] = wi - w;
+        if (lane == 31) *total = wi;
+    }
+    __syncthreads();
+    int r = wsum[warp] + incl - v;
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_reduce(const int *in, int n, int *bsum)
+{
+    __shared__ int wsum[32];
+    __shared__ int total;
+    int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) s += (base + k < n) ? in[base + k] : 0;
+    block_exclusive(s, wsum, &total);
+    if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+}
+
+// single block: exclusive scan of the block sums in place
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_top(int *bsum, int nb)
+{
+    __shared__ int wsum[32];
+    __shared__ int total;
+    int carry = 0;
+    for (int start = 0; start < nb; start += SCAN_TILE) {
+        int base = start + threadIdx.x * SCAN_ITEMS;
+        int v[SCAN_ITEMS];
+        int s = 0;
+#pragma unroll
+        for (int k = 0; k < SCAN_ITEMS; ++k) {
+            v[k] = (base + k < nb) ? bsum[base + k] : 0;
+            s += v[k];
+        }
+        int ex = block_exclusive(s, wsum, &total) + carry;
+#pragma unroll
+        for (int k = 0; k < SCAN_ITEMS; ++k) {
+            if (base + k < nb) bsum[base + k] = ex;
+            ex += v[k];
+        }
+        carry += total;
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(const int *in, int n, const int *bsum, int *out)
+{
+    __shared__ int wsum[32];
+    __shared__ int total;
+    int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+    int v[SCAN_ITEMS];
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        v[k] = (base + k < n) ? in[base + k] : 0;
+        s += v[k];
+    }
+    int ex = block_exclusive(s, wsum, &total) + bsum[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        if (base + k < n) out[base + k] = ex;
+        ex += v[k];
+    }
+}
+
+__global__ void __launch_bounds__(256) k_scatter(BinArgs a)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    int slot = a.cstart[a.cell_of[i]] + a.rank[i];
+    a.sidx[slot] = i;
+    a.spos[slot] = a.pos[i];
+    if (!a.deterministic) a.slot_of[i] = slot;
+}
+
+// per cell: order its points by index (insertion sort; cells hold a handful of points)
+__global__ void __launch_bounds__(256) k_cell_order(BinArgs a)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a.total_cells) return;
+    int lo = a.cstart[c], hi = a.cstart[c + 1];
+    for (int k = lo + 1; k < hi; ++k) {
+        int id = a.sidx[k];
+        double2 ps = a.spos[k];
+        int j = k - 1;
+        while (j >= lo && a.sidx[j] > id) {
+            a.sidx[j + 1] = a.sidx[j];
+            a.spos[j + 1] = a.spos[j];
+            --j;
+        }
+        a.sidx[j + 1] = id;
+        a.spos[j + 1] = ps;
+    }
+    for (int k = lo; k < hi; ++k) a.slot_of[a.sidx[k]] = k;
+}
+
+cudaError_t launch_scan(const int *in, int n, int *bsum, int *out, cudaStream_t s)
+{
+    int nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+    k_scan_reduce<<<nb, SCAN_THREADS, 0, s>>>(in, n, bsum);
+    k_scan_top<<<1, SCAN_THREADS, 0, s>>>(bsum, nb);
+    k_scan_apply<<<nb, SCAN_THREADS, 0, s>>>(in, n, bsum, out);
+    return cudaGetLastError();
+}
+
+int scan_block_count(int n) { return (n + SCAN_TILE - 1) / SCAN_TILE; }
+
+// BinArgs.ccount must hold total_cells + 1 zeros when this is called (the API clears it)
+cudaError_t launch_bin_st(const BinArgs &a, DevStatus *st, cudaStream_t s)
+{
+    if (a.n > 0) k_count<<<(a.n + 255) / 256, 256, 0, s>>>(a, st);
+    cudaError_t e = launch_scan(a.ccount, a.total_cells + 1, a.block_sums, a.cstart, s);
+    if (e != cudaSuccess) return e;
+    if (a.n > 0) k_scatter<<<(a.n + 255) / 256, 256, 0, s>>>(a);
+    if (a.deterministic && a.total_cells > 0) k_cell_order<<<(a.total_cells + 255) / 256, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+// ----------------------------------------------------------------- MD displacement helper
+// x += sigma * N(0,1) per axis, wrapped into the primary cell.  Normals by Box-Muller from a
+// SplitMix64 hash of (seed, step, point); deterministic for given arguments.
+__device__ __forceinline__ unsigned long long smix(unsigned long long z)
+{
+    z += 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ double wrap_coord(double x, double L)
+{
+    if (x >= L) x -= L;
+    else if (x < 0.0) x += L;
+    if (!(x < L)) x = 0.0;   // x + L rounded up to L
+    if (x < 0.0) x = 0.0;
+    return x;
+}
+
+__global__ void __launch_bounds__(256) k_displace(double2 *pos, int n, const SetDesc *sets, const int *set_of,
+                                                  double sigma, unsigned long long seed, unsigned long long step)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const SetDesc &S = sets[set_of ? set_of[i] : 0];
+    unsigned long long h = smix(seed ^ smix(step * 0x100000001B3ULL + (unsigned long long)i));
+    unsigned long long h2 = smix(h);
+    double u1 = ((h >> 11) + 1) * (1.0 / 9007199254740993.0);   // (0, 1]
+    double u2 = (h2 >> 11) * (1.0 / 9007199254740992.0);
+    double r = sigma * sqrt(-2.0 * log(u1));
+    double sn, cs;
+    sincospi(2.0 * u2, &sn, &cs);
+    double2 p = pos[i];
+    p.x = wrap_coord(p.x + r * cs, S.Lx);
+    p.y = wrap_coord(p.y + r * sn, S.Ly);
+    pos[i] = p;
+}
+
+cudaError_t launch_displace(double2 *pos, int n, const SetDesc *sets, const int *set_of, double sigma,
+                            unsigned long long seed, unsigned long long step, cudaStream_t s)
+{
+    if (n <= 0) return cudaSuccess;
+    k_displace<<<(n + 255) / 256, 256, 0, s>>>(pos, n, sets, set_of, sigma, seed, step);
+    return cudaGetLastError();
+}
+
+}  // namespace dgt

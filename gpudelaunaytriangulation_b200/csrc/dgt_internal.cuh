@@ -1,0 +1,139 @@
+// Internal types shared by the binning, ring and API translation units.
+//
+// Data layout in HBM (all arrays device-resident, owned by the context unless noted):
+//   points   double2[n]            caller-owned, original order, primary cell [0,Lx)x[0,Ly)
+//   tri      int[n*stride]         caller-owned; row i holds the CCW ring of point i
+//   nn       int[n]                caller-owned; ring lengths (reference "neighborNum")
+//   cstart   int[cells+1]          CSR cell starts (cells of all sets, set-major)
+//   spos     double2[n]            positions in cell order (coalesced candidate reads)
+//   sidx     int[n]                cell-order slot -> point index
+//   slot_of  int[n]                point index -> cell-order slot
+//   set_of   int[n]                point/slot -> set (batched contexts only, else null)
+// Point indices are global over the concatenated sets; the slots of set s are the range
+// [point_base, point_base + n) because cells are numbered set-major.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace dgt {
+
+struct SetDesc {
+    double Lx, Ly;      // periodic box edges
+    double hLx, hLy;    // half edges (0.5 * L, exact)
+    double icw, ich;    // 1 / cell edge per axis
+    double cw, ch;      // cell edges
+    int xsize, ysize;   // cells per axis (>= 1)
+    int cell_base;      // first cell of the set in cstart
+    int point_base;     // first point / slot of the set
+    int n;              // points in the set
+    float V;            // virtual corner coordinate: power of two >= max(Lx, Ly)
+    int pad;
+};
+
+// device-side status / counters of one call (zeroed at the start of each call)
+struct DevStatus {
+    int need_stride;            // largest ring that did not fit the caller's stride
+    int max_ring;               // largest ring produced
+    int slow_count;             // items queued for the exact/large-capacity kernel
+    int err_flags;              // DGT_EF_* bits
+    int list_count[2];          // repair work lists (ping-pong)
+    int rounds;                 // repair rounds executed (device-side count)
+    int pad;
+    unsigned long long points;          // ring constructions
+    unsigned long long candidates;      // candidates examined
+    unsigned long long tests;           // circle tests evaluated
+    unsigned long long f32_undecided;   // undecided by the float32 filter
+    unsigned long long f64_undecided;   // undecided by the float64 recheck
+    unsigned long long exact_points;    // points run through exact arithmetic
+    unsigned long long capacity_points; // points whose ring outgrew on-chip capacity
+    unsigned long long mismatches;      // check mode: filter decisions contradicted by float64
+    unsigned long long insertions;      // ring insertions
+    unsigned long long flagged;         // points queued by the test kernel
+    unsigned long long repaired;        // points rebuilt by repair rounds
+};
+
+enum : int {
+    EF_UNBOUNDED = 1,      // a ring still held a virtual corner after the whole box was scanned
+    EF_NONCONTIG = 2,      // a conflict set was not one contiguous arc (degenerate input)
+    EF_SLOW_OVERFLOW = 4,  // a ring outgrew even the large-capacity path
+    EF_EXACT_UNRESOLVED = 8,
+    EF_BAD_INPUT = 16,     // coordinates not finite
+};
+
+enum : int { MODE_F32 = 0, MODE_F64 = 1 };
+
+struct BinArgs {
+    const double2 *pos;
+    int n;
+    const SetDesc *sets;
+    const int *set_of;
+    int total_cells;
+    int *ccount;     // total_cells + 1
+    int *cstart;     // total_cells + 1
+    int *cell_of;    // n
+    int *rank;       // n
+    int *sidx, *slot_of;
+    double2 *spos;
+    int *block_sums;
+    int deterministic;
+};
+
+struct RingArgs {
+    const SetDesc *sets;
+    const int *set_of;
+    const double2 *pos;
+    const double2 *spos;
+    const int *sidx;
+    const int *slot_of;
+    const int *cstart;
+    int *tri;
+    int *nn;
+    int stride;
+    int npoints;       // total points (bound for indices read back from caller rows)
+    // work selection: worklist == null -> item t is slot t (t < n_items)
+    const int *worklist;
+    const int *worklist_count;  // device count (used when worklist != null)
+    int n_items;
+    // repair bookkeeping
+    int repair;        // 1: rebuild listed points and propagate consistency checks
+    int *mark;
+    int epoch_base;
+    int epoch;         // mark value of the items of this round; next round uses epoch + 1
+    int *next_list;
+    int *next_count;
+    // deferred items for the exact / large-capacity kernel
+    int *slow_list;
+    int *slow_count;
+    int check;         // 1: count float32 decisions contradicted by float64
+    DevStatus *st;
+};
+
+struct TestArgs {
+    const SetDesc *sets;
+    const int *set_of;
+    const double2 *pos;
+    const int *tri;
+    const int *nn;
+    int stride;
+    int n;
+    int *mark;
+    int epoch_base;
+    int *list;
+    int *list_count;
+    DevStatus *st;
+};
+
+// launchers (defined in the .cu files)
+cudaError_t launch_bin_st(const BinArgs &a, DevStatus *st, cudaStream_t s);
+cudaError_t launch_scan(const int *in, int n, int *bsum, int *out, cudaStream_t s);
+int scan_block_count(int n);
+cudaError_t launch_build(const RingArgs &a, int mode, cudaStream_t s);
+cudaError_t launch_slow(const RingArgs &a, void *scratch, int scratch_items, int capacity, cudaStream_t s);
+cudaError_t launch_test(const TestArgs &a, cudaStream_t s);
+cudaError_t launch_restride(const int *src, int old_stride, int *dst, int new_stride, const int *nn, int n,
+                            cudaStream_t s);
+cudaError_t launch_displace(double2 *pos, int n, const SetDesc *sets, const int *set_of, double sigma,
+                            unsigned long long seed, unsigned long long step, cudaStream_t s);
+size_t slow_scratch_bytes_per_item(int capacity);
+
+}  // namespace dgt

@@ -1,0 +1,691 @@
+// One-ring construction, repair and the local Delaunay test.
+//
+// Per point p (one thread per point, points taken in cell order so a warp works on a compact
+// patch of cells and shares candidate cells through L1):
+//   1. start from a square of four virtual corners (+-V, +-V) (the reference's virtual
+//      polygon, DelaunayGPU.cu:340-351, with V a power of two >= the box so the initial cell
+//      covers every minimum-image offset);
+//   2. insert candidates from p's own cell, then its 3x3 block: a candidate d conflicts with
+//      ring edge (P_k, P_k+1) iff it lies strictly inside the circle through (0, P_k, P_k+1)
+//      (the Voronoi vertex of that edge is on d's side of the bisector, the reference's test
+//      at DelaunayGPU.cu:767-791); the conflicting edges form one arc, whose inner vertices
+//      are replaced by d (DelaunayGPU.cu:795-926 does the same bookkeeping vertex by vertex);
+//   3. certify: every edge circle must lie inside the scanned rectangle of cells; grow the
+//      rectangle one cell per side towards the union of the circles' bounding boxes and
+//      scan the new cells until it does (the reference scans a square spiral around each
+//      Voronoi vertex instead, DelaunayGPU.cu:715-749);
+//   4. write the ring rotated to start at its smallest index (a canonical start; the
+//      reference's start depends on insertion order) into row p of the caller's array.
+// The ring lives in shared memory (per-thread columns, conflict-free).  Points whose ring
+// outgrows that capacity, or that meet a predicate neither float32 nor float64 can decide,
+// are re-run by a large-capacity kernel with exact arithmetic (slow path).
+#include "dgt_internal.cuh"
+#include "dgt_predicates.cuh"
+
+namespace dgt {
+
+enum { R_OK = 0, R_CAPACITY = 1, R_EXACT = 2, R_UNBOUNDED = 3, R_NONCONTIG = 4 };
+
+struct Ctr {
+    unsigned cand, tests, u32, u64, ins, mism;
+};
+
+// ---------------------------------------------------------------- ring storage policies
+template <typename T, int CAP, int BLOCK>
+struct SmemRing {
+    typedef typename Prec<T>::T4 E4;
+    typedef typename Prec<T>::T2 V2;
+    E4 (*e)[BLOCK];
+    V2 (*v)[BLOCK];
+    int (*id)[BLOCK];
+    int t;
+    static constexpr int cap = CAP;
+    __device__ __forceinline__ E4 edge(int k) const { return e[k][t]; }
+    __device__ __forceinline__ V2 vert(int k) const { return v[k][t]; }
+    __device__ __forceinline__ int idx(int k) const { return id[k][t]; }
+    __device__ __forceinline__ void set_edge(int k, E4 x) { e[k][t] = x; }
+    __device__ __forceinline__ void set_vert(int k, V2 x, int i) { v[k][t] = x; id[k][t] = i; }
+    __device__ __forceinline__ void move(int dst, int src)
+    {
+        e[dst][t] = e[src][t];
+        v[dst][t] = v[src][t];
+        id[dst][t] = id[src][t];
+    }
+};
+
+template <typename T, int CAP>
+struct GlobalRing {
+    typedef typename Prec<T>::T4 E4;
+    typedef typename Prec<T>::T2 V2;
+    E4 *e;
+    V2 *v;
+    int *id;
+    static constexpr int cap = CAP;
+    __device__ __forceinline__ E4 edge(int k) const { return e[k]; }
+    __device__ __forceinline__ V2 vert(int k) const { return v[k]; }
+    __device__ __forceinline__ int idx(int k) const { return id[k]; }
+    __device__ __forceinline__ void set_edge(int k, E4 x) { e[k] = x; }
+    __device__ __forceinline__ void set_vert(int k, V2 x, int i) { v[k] = x; id[k] = i; }
+    __device__ __forceinline__ void move(int dst, int src)
+    {
+        e[dst] = e[src];
+        v[dst] = v[src];
+        id[dst] = id[src];
+    }
+};
+
+template <int CAP> struct MaskT { typedef unsigned int type; };
+template <> struct MaskT<64> { typedef unsigned long long type; };
+__device__ __forceinline__ int popc_(unsigned int x) { return __popc(x); }
+__device__ __forceinline__ int popc_(unsigned long long x) { return __popcll(x); }
+__device__ __forceinline__ int ffs_(unsigned int x) { return __ffs(x); }
+__device__ __forceinline__ int ffs_(unsigned long long x) { return __ffsll(x); }
+
+__device__ __forceinline__ int wrapi(int i, int n)
+{
+    int r = i % n;
+    return r < 0 ? r + n : r;
+}
+
+// double offset of ring entry `id` relative to p (virtual corners are exact constants)
+__device__ __forceinline__ double2 entry_off64(const RingArgs &A, const SetDesc &S, double2 p, int id)
+{
+    if (id >= 0) {
+        double2 q = __ldg(&A.pos[id]);
+        return make_double2(wrap_off(q.x, p.x, S.Lx, S.hLx), wrap_off(q.y, p.y, S.Ly, S.hLy));
+    }
+    double V = (double)S.V;
+    int c = -id - 1;   // 0:(V,V) 1:(-V,V) 2:(-V,-V) 3:(V,-V)
+    return make_double2((c == 0 || c == 3) ? V : -V, (c < 2) ? V : -V);
+}
+
+template <typename T>
+__device__ __forceinline__ typename Prec<T>::T2 corner(int c, T V)
+{
+    return Prec<T>::mk2((c == 0 || c == 3) ? V : -V, (c < 2) ? V : -V);
+}
+
+// ------------------------------------------------------------------- the construction
+template <typename T, bool EXACT, class Ring>
+struct Builder {
+    typedef Prec<T> PR;
+    typedef typename PR::T4 E4;
+    typedef typename PR::T2 V2;
+    typedef typename MaskT<Ring::cap>::type Mask;
+
+    const RingArgs &A;
+    const SetDesc &S;
+    Ring &R;
+    Ctr &ctr;
+    double2 p;
+    int slot;
+    int m;
+    T r2max;
+    int ocx, ocy;
+
+    __device__ Builder(const RingArgs &a, const SetDesc &s, Ring &r, Ctr &c, double2 pp, int sl)
+        : A(a), S(s), R(r), ctr(c), p(pp), slot(sl), m(0), r2max((T)0), ocx(0), ocy(0) {}
+
+    __device__ void refresh_r2max()
+    {
+        T mx = (T)0;
+        for (int k = 0; k < m; ++k) {
+            T rc = R.edge(k).w;
+            mx = rc > mx ? rc : mx;
+        }
+        r2max = (T)4 * mx * mx * ((T)1 + (T)64 * PR::u());
+    }
+
+    __device__ void init()
+    {
+        T V = (T)S.V;
+        for (int c = 0; c < 4; ++c) R.set_vert(c, corner<T>(c, V), -1 - c);
+        for (int c = 0; c < 4; ++c) {
+            V2 a = corner<T>(c, V), b = corner<T>((c + 1) & 3, V);
+            R.set_edge(c, make_circ<T>(a.x, a.y, b.x, b.y));
+        }
+        m = 4;
+        refresh_r2max();
+        int cx = (int)floor(p.x * S.icw), cy = (int)floor(p.y * S.ich);
+        ocx = min(max(cx, 0), S.xsize - 1);
+        ocy = min(max(cy, 0), S.ysize - 1);
+    }
+
+    // float64 (then exact) decision for edge k against candidate d; +1 conflict, -1 none,
+    // 0 undecided (only without EXACT)
+    __device__ int recheck(int k, double2 d64)
+    {
+        int ia = R.idx(k), ib = R.idx(k + 1 == m ? 0 : k + 1);
+        double2 a = entry_off64(A, S, p, ia), b = entry_off64(A, S, p, ib);
+        int r = incircle64(a.x, a.y, b.x, b.y, d64.x, d64.y);
+        if (r != 0) return r;
+        ctr.u64++;
+        if (EXACT) {
+            r = incircle_exact(a.x, a.y, b.x, b.y, d64.x, d64.y);
+            return r > 0 ? 1 : -1;   // on the circle: not strictly inside
+        }
+        return 0;
+    }
+
+    __device__ int insert(V2 d, int id, Mask mask)
+    {
+        Mask full = (m == 64) ? ~(Mask)0 : (((Mask)1 << m) - 1);
+        Mask nm = ~mask & full;
+        Mask rl = ((nm << 1) | (nm >> (m - 1))) & full;
+        Mask rr = ((nm >> 1) | (nm << (m - 1))) & full;
+        Mask starts = mask & rl, ends = mask & rr;
+        if (mask == full || popc_(starts) != 1) return R_NONCONTIG;
+        int s = ffs_(starts) - 1, e = ffs_(ends) - 1, c = popc_(mask);
+        int mnew = m - c + 2;
+        if (mnew > Ring::cap) return R_CAPACITY;
+        V2 vs = R.vert(s), ve = R.vert(e + 1 == m ? 0 : e + 1);
+        E4 ca = make_circ<T>(vs.x, vs.y, d.x, d.y);
+        E4 cb = make_circ<T>(d.x, d.y, ve.x, ve.y);
+        int ns;
+        if (s <= e) {
+            int delta = 2 - c;
+            if (delta > 0) {
+                for (int k = m - 1; k >= e + 1; --k) R.move(k + 1, k);
+            } else if (delta < 0) {
+                for (int k = e + 1; k < m; ++k) R.move(k + delta, k);
+            }
+            ns = s;
+        } else {
+            for (int k = e + 1; k <= s; ++k) R.move(k - (e + 1), k);
+            ns = s - e - 1;
+        }
+        R.set_edge(ns, ca);
+        R.set_vert(ns + 1, d, id);
+        R.set_edge(ns + 1, cb);
+        m = mnew;
+        ctr.ins++;
+        refresh_r2max();
+        return R_OK;
+    }
+
+    __device__ int scan_cell(int rx, int ry)
+    {
+        int cx = wrapi(ocx + rx, S.xsize), cy = wrapi(ocy + ry, S.ysize);
+        int c = S.cell_base + cy * S.xsize + cx;
+        int a = __ldg(&A.cstart[c]), b = __ldg(&A.cstart[c + 1]);
+        const T u = PR::u();
+        for (int sl = a; sl < b; ++sl) {
+            if (sl == slot) continue;
+            double2 q = __ldg(&A.spos[sl]);
+            double2 d64 = make_double2(wrap_off(q.x, p.x, S.Lx, S.hLx), wrap_off(q.y, p.y, S.Ly, S.hLy));
+            if (d64.x == 0.0 && d64.y == 0.0) continue;   // coincident point
+            ctr.cand++;
+            V2 d = PR::mk2(PR::from64(d64.x), PR::from64(d64.y));
+            T nd = d.x * d.x + d.y * d.y;
+            if (nd > r2max) continue;
+            T ad = sqrt(nd);
+            T kb = (T)8 * u * nd + PR::tiny();
+            Mask mask = 0;
+            for (int k = 0; k < m; ++k) {
+                E4 e = R.edge(k);
+                T sv = fma(d.x, e.x, fma(d.y, e.y, -nd));
+                T bd = fma(ad, e.z, kb);
+                ctr.tests++;
+                if (sv > bd) {
+                    mask |= (Mask)1 << k;
+                    if (A.check) {
+                        int ia = R.idx(k), ib = R.idx(k + 1 == m ? 0 : k + 1);
+                        double2 aa = entry_off64(A, S, p, ia), bb = entry_off64(A, S, p, ib);
+                        if (incircle64(aa.x, aa.y, bb.x, bb.y, d64.x, d64.y) < 0) ctr.mism++;
+                    }
+                } else if (sv >= -bd) {
+                    ctr.u32++;
+                    int r = recheck(k, d64);
+                    if (r == 0) return R_EXACT;
+                    if (r > 0) mask |= (Mask)1 << k;
+                } else if (A.check) {
+                    int ia = R.idx(k), ib = R.idx(k + 1 == m ? 0 : k + 1);
+                    double2 aa = entry_off64(A, S, p, ia), bb = entry_off64(A, S, p, ib);
+                    if (incircle64(aa.x, aa.y, bb.x, bb.y, d64.x, d64.y) > 0) ctr.mism++;
+                }
+            }
+            if (!mask) continue;
+            int r = insert(d, __ldg(&A.sidx[sl]), mask);
+            if (r != R_OK) return r;
+        }
+        return R_OK;
+    }
+
+    // scan the cells of [nx0,nx1]x[ny0,ny1] that are not in [x0,x1]x[y0,y1]
+    __device__ int scan_growth(int x0, int x1, int y0, int y1, int nx0, int nx1, int ny0, int ny1)
+    {
+        int r;
+        for (int x = nx0; x < x0; ++x)
+            for (int y = y0; y <= y1; ++y)
+                if ((r = scan_cell(x, y)) != R_OK) return r;
+        for (int x = x1 + 1; x <= nx1; ++x)
+            for (int y = y0; y <= y1; ++y)
+                if ((r = scan_cell(x, y)) != R_OK) return r;
+        for (int y = ny0; y < y0; ++y)
+            for (int x = nx0; x <= nx1; ++x)
+                if ((r = scan_cell(x, y)) != R_OK) return r;
+        for (int y = y1 + 1; y <= ny1; ++y)
+            for (int x = nx0; x <= nx1; ++x)
+                if ((r = scan_cell(x, y)) != R_OK) return r;
+        return R_OK;
+    }
+
+    // circle of edge k in double: centre (relative) and safe radius; false if degenerate
+    __device__ bool circle64(int k, double &cx, double &cy, double &rc)
+    {
+        int ia = R.idx(k), ib = R.idx(k + 1 == m ? 0 : k + 1);
+        double2 a = entry_off64(A, S, p, ia), b = entry_off64(A, S, p, ib);
+        double4 c = make_circ<double>(a.x, a.y, b.x, b.y);
+        if (!(c.w < Prec<double>::inf())) return false;
+        cx = 0.5 * c.x;
+        cy = 0.5 * c.y;
+        rc = c.w;
+        return true;
+    }
+
+    __device__ int run()
+    {
+        init();
+        int r = scan_cell(0, 0);
+        if (r != R_OK) return r;
+        int x0 = 0, x1 = 0, y0 = 0, y1 = 0;
+        // the 3x3 block (fewer columns/rows on grids narrower than 3 cells)
+        int nx0 = S.xsize >= 3 ? -1 : 0, nx1 = S.xsize >= 2 ? 1 : 0;
+        int ny0 = S.ysize >= 3 ? -1 : 0, ny1 = S.ysize >= 2 ? 1 : 0;
+        r = scan_growth(x0, x1, y0, y1, nx0, nx1, ny0, ny1);
+        if (r != R_OK) return r;
+        x0 = nx0; x1 = nx1; y0 = ny0; y1 = ny1;
+        const double fx = p.x * S.icw - (double)ocx, fy = p.y * S.ich - (double)ocy;
+        for (int it = 0; it < S.xsize + S.ysize + 8; ++it) {
+            // union of the edge circles' bounding boxes, in cells relative to the own cell
+            double xmin = 1e300, xmax = -1e300, ymin = 1e300, ymax = -1e300;
+            bool full = false;
+            for (int k = 0; k < m && !full; ++k) {
+                E4 e = R.edge(k);
+                double cx, cy, rc;
+                if (e.w < PR::inf()) {
+                    cx = 0.5 * (double)e.x;
+                    cy = 0.5 * (double)e.y;
+                    rc = (double)e.w;
+                } else if (!circle64(k, cx, cy, rc)) {
+                    full = true;
+                    break;
+                }
+                xmin = fmin(xmin, cx - rc);
+                xmax = fmax(xmax, cx + rc);
+                ymin = fmin(ymin, cy - rc);
+                ymax = fmax(ymax, cy + rc);
+            }
+            int lx, hx, ly, hy;
+            if (full) {
+                lx = ly = -(1 << 28);
+                hx = hy = (1 << 28);
+            } else {
+                double a0 = fx + xmin * S.icw, a1 = fx + xmax * S.icw;
+                double b0 = fy + ymin * S.ich, b1 = fy + ymax * S.ich;
+                a0 -= 1e-9 * (1.0 + fabs(a0));
+                a1 += 1e-9 * (1.0 + fabs(a1));
+                b0 -= 1e-9 * (1.0 + fabs(b0));
+                b1 += 1e-9 * (1.0 + fabs(b1));
+                lx = (int)fmax(floor(a0), -1e8);
+                hx = (int)fmin(floor(a1), 1e8);
+                ly = (int)fmax(floor(b0), -1e8);
+                hy = (int)fmin(floor(b1), 1e8);
+            }
+            int gx0 = x0, gx1 = x1, gy0 = y0, gy1 = y1;
+            if (lx < x0 && gx1 - gx0 + 1 < S.xsize) gx0--;
+            if (hx > x1 && gx1 - gx0 + 1 < S.xsize) gx1++;
+            if (ly < y0 && gy1 - gy0 + 1 < S.ysize) gy0--;
+            if (hy > y1 && gy1 - gy0 + 1 < S.ysize) gy1++;
+            if (gx0 == x0 && gx1 == x1 && gy0 == y0 && gy1 == y1) break;
+            r = scan_growth(x0, x1, y0, y1, gx0, gx1, gy0, gy1);
+            if (r != R_OK) return r;
+            x0 = gx0; x1 = gx1; y0 = gy0; y1 = gy1;
+        }
+        for (int k = 0; k < m; ++k)
+            if (R.idx(k) < 0) return R_UNBOUNDED;
+        return R_OK;
+    }
+};
+
+// ------------------------------------------------------------- output + repair bookkeeping
+__device__ __forceinline__ void enqueue_next(const RingArgs &A, int j)
+{
+    if (atomicMax(&A.mark[j], A.epoch + 1) < A.epoch_base) A.next_list[atomicAdd(A.next_count, 1)] = j;
+}
+
+template <class Ring>
+__device__ void finish(const RingArgs &A, int pid, Ring &R, int m, int &maxr)
+{
+    maxr = max(maxr, m);
+    int *row = A.tri + (size_t)pid * A.stride;
+    if (A.repair) {
+        // consistency of the rebuilt ring with the rings it touches (see enqueue rules in
+        // dgt_api.cu: points rebuilt in this call are exact; an untouched point must either
+        // list pid with the matching neighbours on both sides or be rebuilt too)
+        int om = A.nn[pid];
+        if (om >= 1 && om <= A.stride) {
+            for (int k = 0; k < om; ++k) {
+                int o = row[k];
+                bool kept = false;
+                for (int t = 0; t < m; ++t) kept |= (R.idx(t) == o);
+                if (!kept && o >= 0 && o < A.npoints) enqueue_next(A, o);
+            }
+        }
+        for (int k = 0; k < m; ++k) {
+            int nb = R.idx(k);
+            if (A.mark[nb] >= A.epoch_base) continue;
+            int pred = R.idx(k == 0 ? m - 1 : k - 1), succ = R.idx(k + 1 == m ? 0 : k + 1);
+            int mn = A.nn[nb];
+            bool ok = (mn >= 3 && mn <= A.stride);
+            if (ok) {
+                const int *rn = A.tri + (size_t)nb * A.stride;
+                int pos = -1;
+                for (int t = 0; t < mn; ++t)
+                    if (rn[t] == pid) pos = t;
+                ok = pos >= 0 && rn[pos == 0 ? mn - 1 : pos - 1] == succ && rn[pos + 1 == mn ? 0 : pos + 1] == pred;
+            }
+            if (!ok) enqueue_next(A, nb);
+        }
+    }
+    if (m > A.stride) {
+        atomicMax(&A.st->need_stride, m);
+        A.nn[pid] = 0;   // row left unwritten: mark the ring invalid
+        return;
+    }
+    int best = 0, bv = R.idx(0);
+    for (int k = 1; k < m; ++k) {
+        int v = R.idx(k);
+        if (v < bv) { bv = v; best = k; }
+    }
+    for (int k = 0; k < m; ++k) {
+        int src = best + k;
+        if (src >= m) src -= m;
+        row[k] = R.idx(src);
+    }
+    A.nn[pid] = m;
+}
+
+__device__ __forceinline__ void flush_counters(const RingArgs &A, const Ctr &c, unsigned pts, int maxr)
+{
+    unsigned long long v[7] = { pts, c.cand, c.tests, c.u32, c.u64, c.ins, c.mism };
+    for (int i = 0; i < 7; ++i)
+        for (int o = 16; o > 0; o >>= 1) v[i] += __shfl_down_sync(0xffffffffu, v[i], o);
+    for (int o = 16; o > 0; o >>= 1) maxr = max(maxr, __shfl_down_sync(0xffffffffu, maxr, o));
+    if ((threadIdx.x & 31) == 0) {
+        if (v[0]) atomicAdd(&A.st->points, v[0]);
+        if (v[1]) atomicAdd(&A.st->candidates, v[1]);
+        if (v[2]) atomicAdd(&A.st->tests, v[2]);
+        if (v[3]) atomicAdd(&A.st->f32_undecided, v[3]);
+        if (v[4]) atomicAdd(&A.st->f64_undecided, v[4]);
+        if (v[5]) atomicAdd(&A.st->insertions, v[5]);
+        if (v[6]) atomicAdd(&A.st->mismatches, v[6]);
+        if (maxr > 0) atomicMax(&A.st->max_ring, maxr);
+    }
+}
+
+__device__ __forceinline__ int item_count(const RingArgs &A)
+{
+    if (!A.worklist) return A.n_items;
+    int c = *A.worklist_count;
+    return c < A.n_items ? c : A.n_items;
+}
+
+// hot kernel: shared-memory ring of CAP entries per thread
+template <typename T, int CAP, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_build(RingArgs A)
+{
+    typedef typename Prec<T>::T4 E4;
+    typedef typename Prec<T>::T2 V2;
+    __shared__ E4 se[CAP][BLOCK];
+    __shared__ V2 sv[CAP][BLOCK];
+    __shared__ int si[CAP][BLOCK];
+    SmemRing<T, CAP, BLOCK> ring{ se, sv, si, (int)threadIdx.x };
+    Ctr ctr = { 0, 0, 0, 0, 0, 0 };
+    unsigned pts = 0;
+    int maxr = 0;
+    const int n = item_count(A);
+    if (A.repair && blockIdx.x == 0 && threadIdx.x == 0 && n > 0) {
+        atomicAdd(&A.st->repaired, (unsigned long long)n);
+        atomicMax(&A.st->rounds, A.epoch - A.epoch_base + 1);
+    }
+    for (int base = blockIdx.x * BLOCK; base < n; base += gridDim.x * BLOCK) {
+        int t = base + threadIdx.x;
+        if (t < n) {
+            int pid, slot;
+            if (A.worklist) {
+                pid = A.worklist[t];
+                slot = A.slot_of[pid];
+            } else {
+                slot = t;
+                pid = __ldg(&A.sidx[t]);
+            }
+            const SetDesc S = A.sets[A.set_of ? __ldg(&A.set_of[slot]) : 0];
+            double2 p = __ldg(&A.spos[slot]);
+            Builder<T, false, SmemRing<T, CAP, BLOCK>> b(A, S, ring, ctr, p, slot);
+            int r = b.run();
+            pts++;
+            if (r == R_OK) {
+                finish(A, pid, ring, b.m, maxr);
+            } else if (r == R_CAPACITY || r == R_EXACT) {
+                A.slow_list[atomicAdd(A.slow_count, 1)] = pid;
+            } else {
+                atomicOr(&A.st->err_flags, r == R_UNBOUNDED ? EF_UNBOUNDED : EF_NONCONTIG);
+                A.nn[pid] = 0;
+            }
+        }
+    }
+    flush_counters(A, ctr, pts, maxr);
+}
+
+// slow kernel: double + exact arithmetic, ring of 64 entries in a global scratch row per
+// thread; grid-stride over the device-side slow list
+constexpr int SLOW_CAP = 64;
+
+template <typename T>
+struct SlowRow {
+    typename Prec<T>::T4 e[SLOW_CAP];
+    typename Prec<T>::T2 v[SLOW_CAP];
+    int id[SLOW_CAP];
+};
+
+__global__ void __launch_bounds__(64) k_build_slow(RingArgs A, SlowRow<double> *scratch, int scratch_items)
+{
+    int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    Ctr ctr = { 0, 0, 0, 0, 0, 0 };
+    unsigned pts = 0;
+    int maxr = 0;
+    const int n = *A.slow_count;
+    const int nthreads = gridDim.x * blockDim.x;
+    const int rounds = (n + nthreads - 1) / nthreads;
+    for (int rd = 0; rd < rounds; ++rd) {
+        int t = rd * nthreads + tid;
+        if (t < n && tid < scratch_items) {
+            int pid = A.slow_list[t];
+            int slot = A.slot_of[pid];
+            const SetDesc S = A.sets[A.set_of ? A.set_of[slot] : 0];
+            double2 p = A.spos[slot];
+            SlowRow<double> &row = scratch[tid];
+            GlobalRing<double, SLOW_CAP> ring{ row.e, row.v, row.id };
+            Builder<double, true, GlobalRing<double, SLOW_CAP>> b(A, S, ring, ctr, p, slot);
+            int r = b.run();
+            pts++;
+            if (r == R_OK) {
+                finish(A, pid, ring, b.m, maxr);
+            } else {
+                atomicOr(&A.st->err_flags, r == R_CAPACITY ? EF_SLOW_OVERFLOW
+                                          : r == R_UNBOUNDED ? EF_UNBOUNDED
+                                          : r == R_NONCONTIG ? EF_NONCONTIG : EF_EXACT_UNRESOLVED);
+                A.nn[pid] = 0;
+            }
+        }
+    }
+    if (pts) atomicAdd(&A.st->exact_points, (unsigned long long)pts);
+    flush_counters(A, ctr, 0, maxr);
+}
+
+size_t slow_scratch_bytes_per_item(int) { return sizeof(SlowRow<double>); }
+
+// ------------------------------------------------------------------ local Delaunay test
+// Flags every point whose fan is not certainly a piece of the Delaunay triangulation:
+// a fan triangle that is not strictly CCW, a fan that does not wind exactly once, or a
+// spoke (p, P_k) whose opposite vertex P_k+1 is not certainly outside the circle through
+// (p, P_k-1, P_k).  The four vertices of a failing spoke's quadrilateral are queued (an
+// edge flip changes all four rings).  Undecided filters count as failures.
+__device__ __forceinline__ void warp_append(int *list, int *count, const int *items, int k)
+{
+    const int lane = threadIdx.x & 31;
+    int incl = k;
+    for (int o = 1; o < 32; o <<= 1) {
+        int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    int total = __shfl_sync(0xffffffffu, incl, 31);
+    int base = 0;
+    if (lane == 31 && total > 0) base = atomicAdd(count, total);
+    base = __shfl_sync(0xffffffffu, base, 31);
+    int off = base + incl - k;
+    for (int i = 0; i < k; ++i) list[off + i] = items[i];
+}
+
+constexpr int TEST_MAX_QUEUE = 24;
+
+__global__ void __launch_bounds__(256) k_test(TestArgs A)
+{
+    unsigned long long flagged = 0;
+    for (int base = blockIdx.x * blockDim.x; base < A.n; base += gridDim.x * blockDim.x) {
+        int i = base + threadIdx.x;
+        int q[TEST_MAX_QUEUE];
+        int nq = 0;
+        if (i < A.n) {
+            int m = A.nn[i];
+            bool bad = (m < 3 || m > A.stride);
+            const int *row = A.tri + (size_t)i * A.stride;
+            int fail_k[3] = { -1, -1, -1 };
+            int nf = 0;
+            if (!bad) {
+                for (int k = 0; k < m; ++k) {
+                    int r = row[k];
+                    if (r < 0 || r >= A.n || r == i) bad = true;
+                }
+            }
+            if (!bad) {
+                const SetDesc S = A.sets[A.set_of ? A.set_of[i] : 0];
+                double2 p = A.pos[i];
+                double2 q0 = __ldg(&A.pos[row[0]]), ql = __ldg(&A.pos[row[m - 1]]);
+                double2 o0 = make_double2(wrap_off(q0.x, p.x, S.Lx, S.hLx), wrap_off(q0.y, p.y, S.Ly, S.hLy));
+                double2 prev = make_double2(wrap_off(ql.x, p.x, S.Lx, S.hLx), wrap_off(ql.y, p.y, S.Ly, S.hLy));
+                double2 cur = o0;
+                int cross = 0;
+                for (int k = 0; k < m; ++k) {
+                    double2 nxt;
+                    if (k + 1 < m) {
+                        double2 qn = __ldg(&A.pos[row[k + 1]]);
+                        nxt = make_double2(wrap_off(qn.x, p.x, S.Lx, S.hLx), wrap_off(qn.y, p.y, S.Ly, S.hLy));
+                    } else {
+                        nxt = o0;
+                    }
+                    // triangle (p, P_k, P_k+1) strictly CCW
+                    int o = orient32(__double2float_rn(cur.x), __double2float_rn(cur.y), __double2float_rn(nxt.x),
+                                     __double2float_rn(nxt.y));
+                    if (o == 0) o = orient64(cur.x, cur.y, nxt.x, nxt.y);
+                    // spoke (p, P_k): P_k+1 outside circle (p, P_k-1, P_k)
+                    int ic = incircle32(__double2float_rn(prev.x), __double2float_rn(prev.y), __double2float_rn(cur.x),
+                                        __double2float_rn(cur.y), __double2float_rn(nxt.x), __double2float_rn(nxt.y));
+                    if (ic == 0) ic = incircle64(prev.x, prev.y, cur.x, cur.y, nxt.x, nxt.y);
+                    if (cur.y < 0.0 && nxt.y >= 0.0) cross++;
+                    if (o <= 0 || ic >= 0) {
+                        if (nf < 3) fail_k[nf] = k;
+                        nf++;
+                    }
+                    prev = cur;
+                    cur = nxt;
+                }
+                if (cross != 1) bad = true;
+            }
+            if (bad || nf > 0) {
+                if (atomicMax(&A.mark[i], A.epoch_base) < A.epoch_base) q[nq++] = i;
+                if (!bad) {
+                    // a spoke failure: its quadrilateral; more than three failures: the whole fan
+                    if (nf <= 3) {
+                        for (int f = 0; f < nf; ++f) {
+                            int k = fail_k[f];
+                            int js[3] = { row[k == 0 ? m - 1 : k - 1], row[k], row[k + 1 == m ? 0 : k + 1] };
+                            for (int t = 0; t < 3; ++t)
+                                if (nq < TEST_MAX_QUEUE && atomicMax(&A.mark[js[t]], A.epoch_base) < A.epoch_base)
+                                    q[nq++] = js[t];
+                        }
+                    } else {
+                        for (int k = 0; k < m; ++k)
+                            if (nq < TEST_MAX_QUEUE && atomicMax(&A.mark[row[k]], A.epoch_base) < A.epoch_base)
+                                q[nq++] = row[k];
+                    }
+                }
+            }
+        }
+        flagged += nq;
+        warp_append(A.list, A.list_count, q, nq);
+    }
+    for (int o = 16; o > 0; o >>= 1) flagged += __shfl_down_sync(0xffffffffu, flagged, o);
+    if ((threadIdx.x & 31) == 0 && flagged) atomicAdd(&A.st->flagged, flagged);
+}
+
+// ------------------------------------------------------------------------- launchers
+template <typename T, int CAP, int BLOCK>
+static cudaError_t launch_build_t(const RingArgs &a, cudaStream_t s)
+{
+    int blocks;
+    if (a.worklist) {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        int want = (a.n_items + BLOCK - 1) / BLOCK;
+        blocks = want < sms * 32 ? want : sms * 32;
+    } else {
+        blocks = (a.n_items + BLOCK - 1) / BLOCK;
+    }
+    if (blocks < 1) blocks = 1;
+    k_build<T, CAP, BLOCK><<<blocks, BLOCK, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_build(const RingArgs &a, int mode, cudaStream_t s)
+{
+    if (a.n_items <= 0) return cudaSuccess;
+    if (mode == MODE_F64) return launch_build_t<double, 14, 64>(a, s);
+    return launch_build_t<float, 14, 64>(a, s);
+}
+
+cudaError_t launch_slow(const RingArgs &a, void *scratch, int scratch_items, int, cudaStream_t s)
+{
+    int blocks = (scratch_items + 63) / 64;
+    if (blocks < 1) blocks = 1;
+    k_build_slow<<<blocks, 64, 0, s>>>(a, reinterpret_cast<SlowRow<double> *>(scratch), scratch_items);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_test(const TestArgs &a, cudaStream_t s)
+{
+    if (a.n <= 0) return cudaSuccess;
+    int blocks = (a.n + 255) / 256;
+    k_test<<<blocks, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+__global__ void k_restride(const int *src, int os, int *dst, int ns, const int *nn, int n)
+{
+    int i = blockIdx.y * gridDim.x + blockIdx.x;
+    if (i >= n) return;
+    int m = nn ? min(nn[i], min(os, ns)) : min(os, ns);
+    for (int k = threadIdx.x; k < ns; k += blockDim.x) dst[(size_t)i * ns + k] = k < m ? src[(size_t)i * os + k] : 0;
+}
+
+cudaError_t launch_restride(const int *src, int os, int *dst, int ns, const int *nn, int n, cudaStream_t s)
+{
+    if (n <= 0) return cudaSuccess;
+    dim3 g(n < 65535 ? n : 65535, (n + 65534) / 65535);
+    k_restride<<<g, 32, 0, s>>>(src, os, dst, ns, nn, n);
+    return cudaGetLastError();
+}
+
+}  // namespace dgt

@@ -1,0 +1,230 @@
+"""Python mirror of the reference's DelaunayGPU class (src/model/DelaunayGPU.h:18-130) over
+the C ABI.  Device memory is held in torch CUDA tensors (plumbing only); every call goes to
+libdgt.so and fails loudly when the library or a GPU is missing.
+
+    box = PeriodicBox(L, L)
+    delGPU = DelaunayGPU(N, maxNeighs, cellSize, box)             # DelaunayGPU.h:25
+    tri = torch.zeros(maxNeighs * N, dtype=torch.int32, device="cuda")
+    nn = torch.zeros(N, dtype=torch.int32, device="cuda")
+    delGPU.globalDelaunayTriangulation(pts, tri, nn)              # DelaunayGPU.h:30
+    delGPU.testAndRepairDelaunayTriangulation(pts, tri, nn)       # DelaunayGPU.h:33
+
+As in the reference the callee may resize the caller's triangulation array to MaxSize*N
+(DelaunayGPU.cpp:126-132, :152-155); the row stride is tri.numel() // N.  With safety mode
+off an overflowing ring raises instead of silently corrupting the output (the reference's
+GPU path returns early without writing, DelaunayGPU.cu:874-879).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import torch
+
+from . import _native as N
+
+
+@dataclass
+class PeriodicBox:
+    """Rectangular periodic box [0, Lx) x [0, Ly) (periodicBoundaries(x, y),
+    src/utilities/periodicBoundaries.h:30)."""
+
+    Lx: float
+    Ly: float
+
+    def putInBoxReal(self, p: torch.Tensor) -> torch.Tensor:
+        """Wrap points into the primary cell (periodicBoundaries.h:131-152)."""
+        out = p.clone()
+        out[..., 0] = torch.remainder(out[..., 0], self.Lx)
+        out[..., 1] = torch.remainder(out[..., 1], self.Ly)
+        out[..., 0] = torch.where(out[..., 0] >= self.Lx, torch.zeros_like(out[..., 0]), out[..., 0])
+        out[..., 1] = torch.where(out[..., 1] >= self.Ly, torch.zeros_like(out[..., 1]), out[..., 1])
+        return out
+
+
+def _ptr(t: torch.Tensor | None):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+def _check_points(points: torch.Tensor, n: int):
+    if not (isinstance(points, torch.Tensor) and points.is_cuda):
+        raise TypeError("points must be a CUDA tensor")
+    if points.dtype != torch.float64 or points.numel() != 2 * n or not points.is_contiguous():
+        raise ValueError(f"points must be a contiguous float64 CUDA tensor of {n} x 2 values")
+
+
+def _check_int(t: torch.Tensor, name: str):
+    if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.int32 and t.is_contiguous()):
+        raise TypeError(f"{name} must be a contiguous int32 CUDA tensor")
+
+
+class DelaunayGPU:
+    """Per-point periodic Delaunay one-rings on the GPU (reference API names kept)."""
+
+    def __init__(self, N: int, maximumNeighborsGuess: int = 16, cellSize: float = 1.0,
+                 box: PeriodicBox | tuple | None = None, *, _batch=None):
+        self._L = N_lib = N.lib()
+        self._h = ctypes.c_void_p()
+        if _batch is not None:
+            sizes, boxes, rel_cell = _batch
+            sz = (ctypes.c_int * len(sizes))(*[int(s) for s in sizes])
+            bx = (ctypes.c_double * (2 * len(sizes)))(*[float(v) for b in boxes for v in b])
+            N.check(N_lib.dgt_create_batch(len(sizes), sz, bx, float(rel_cell), int(maximumNeighborsGuess),
+                                           ctypes.byref(self._h)), "dgt_create_batch")
+            self.Ncells = int(sum(int(s) for s in sizes))
+            self.Box = None
+        else:
+            if box is None:
+                raise ValueError("a periodic box is required")
+            if not isinstance(box, PeriodicBox):
+                box = PeriodicBox(float(box[0]), float(box[1]))
+            self.Box = box
+            self.Ncells = int(N)
+            N.check(N_lib.dgt_create(self.Ncells, int(maximumNeighborsGuess), float(cellSize), box.Lx, box.Ly,
+                                     ctypes.byref(self._h)), "dgt_create")
+        self.safetyMode = True
+        self.GPUcompute = True
+        self.last_stats: dict | None = None
+
+    # ------------------------------------------------------------------ reference setters
+    @property
+    def MaxSize(self) -> int:
+        v = ctypes.c_int()
+        N.check(self._L.dgt_get_max_size(self._h, ctypes.byref(v)), "dgt_get_max_size")
+        return v.value
+
+    def resize(self, nmax: int):
+        """resize(nmax) (DelaunayGPU.h:38): the ring capacity MaxSize."""
+        N.check(self._L.dgt_resize(self._h, int(nmax)), "dgt_resize")
+
+    def setCellListSize(self, csize: float):
+        N.check(self._L.dgt_set_cell_size(self._h, float(csize)), "dgt_set_cell_size")
+
+    def setBox(self, box: PeriodicBox | tuple):
+        if not isinstance(box, PeriodicBox):
+            box = PeriodicBox(float(box[0]), float(box[1]))
+        N.check(self._L.dgt_set_box(self._h, box.Lx, box.Ly), "dgt_set_box")
+        self.Box = box
+
+    def setSafetyMode(self, flag: bool):
+        self.safetyMode = bool(flag)
+        N.check(self._L.dgt_set_safety_mode(self._h, 1 if flag else 0), "dgt_set_safety_mode")
+
+    def setGPUcompute(self, flag: bool):
+        """The reference can run its OpenMP host path instead; this library has no CPU path."""
+        if not flag:
+            raise NotImplementedError("no CPU path: the triangulation always runs on the GPU")
+        self.GPUcompute = True
+
+    def setOMPthreads(self, num: int):
+        """Accepted for API compatibility; there is no host path to thread."""
+        return None
+
+    def setPrecision(self, fp32_filter: bool = True):
+        N.check(self._L.dgt_set_precision(self._h, N.PRECISION_FP32_FILTER if fp32_filter else N.PRECISION_FP64),
+                "dgt_set_precision")
+
+    def setCheckMode(self, on: bool):
+        N.check(self._L.dgt_set_check_mode(self._h, 1 if on else 0), "dgt_set_check_mode")
+
+    # ------------------------------------------------------------------------- the path
+    def updateList(self, points: torch.Tensor, stream=None):
+        _check_points(points, self.Ncells)
+        N.check(self._L.dgt_update_list(self._h, _ptr(points), _stream_ptr(stream)), "dgt_update_list")
+
+    def _fit(self, tri: torch.Tensor | None, nn: torch.Tensor | None, device):
+        n = self.Ncells
+        if tri is None:
+            tri = torch.zeros(self.MaxSize * n, dtype=torch.int32, device=device)
+        if nn is None:
+            nn = torch.zeros(n, dtype=torch.int32, device=device)
+        _check_int(tri, "GPUTriangulation")
+        _check_int(nn, "cellNeighborNum")
+        if nn.numel() != n:
+            nn.resize_(n)
+        if n and (tri.numel() % n != 0 or tri.numel() // n < self.MaxSize):
+            tri.resize_(self.MaxSize * n)
+        return tri, nn
+
+    def globalDelaunayTriangulation(self, points: torch.Tensor, GPUTriangulation: torch.Tensor | None = None,
+                                    cellNeighborNum: torch.Tensor | None = None, stream=None):
+        n = self.Ncells
+        _check_points(points, n)
+        tri, nn = self._fit(GPUTriangulation, cellNeighborNum, points.device)
+        if n == 0:
+            return tri, nn
+        while True:
+            stride = tri.numel() // n
+            code = self._L.dgt_global_triangulation(self._h, _ptr(points), _ptr(tri), _ptr(nn), stride,
+                                                    _stream_ptr(stream))
+            if code == N.DGT_ERR_NEED_RESIZE and self.safetyMode:
+                tri.resize_(self.MaxSize * n)   # DelaunayGPU.cpp:152-155 grows and recomputes
+                continue
+            N.check(code, "globalDelaunayTriangulation")
+            break
+        return tri, nn
+
+    def testAndRepairDelaunayTriangulation(self, points: torch.Tensor, GPUTriangulation: torch.Tensor,
+                                           cellNeighborNum: torch.Tensor, stream=None):
+        n = self.Ncells
+        _check_points(points, n)
+        _check_int(GPUTriangulation, "GPUTriangulation")
+        _check_int(cellNeighborNum, "cellNeighborNum")
+        if n == 0:
+            return GPUTriangulation, cellNeighborNum
+        tri, nn = GPUTriangulation, cellNeighborNum
+        while True:
+            stride = tri.numel() // n
+            code = self._L.dgt_test_and_repair(self._h, _ptr(points), _ptr(tri), _ptr(nn), stride,
+                                               _stream_ptr(stream))
+            if code == N.DGT_ERR_NEED_RESIZE and self.safetyMode:
+                # re-stride every row into the larger array (rows keep their contents;
+                # the reference copies linearly here, DelaunayGPU.cpp:109-112), then go on
+                new = torch.zeros(self.MaxSize * n, dtype=torch.int32, device=tri.device)
+                N.check(self._L.dgt_restride(_ptr(tri), stride, _ptr(new), self.MaxSize, _ptr(nn), n,
+                                             _stream_ptr(stream)), "dgt_restride")
+                tri.resize_(new.numel())
+                tri.copy_(new)
+                continue
+            N.check(code, "testAndRepairDelaunayTriangulation")
+            break
+        return tri, nn
+
+    def displace(self, points: torch.Tensor, sigma: float, seed: int, step: int, stream=None):
+        """MD-like step helper: Gaussian displacement + periodic wrap on the device."""
+        _check_points(points, self.Ncells)
+        N.check(self._L.dgt_displace(self._h, _ptr(points), float(sigma), int(seed) & (2**64 - 1),
+                                     int(step) & (2**64 - 1), _stream_ptr(stream)), "dgt_displace")
+
+    def stats(self) -> dict:
+        s = N.Stats()
+        N.check(self._L.dgt_get_stats(self._h, ctypes.byref(s)), "dgt_get_stats")
+        self.last_stats = s.as_dict()
+        return self.last_stats
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._L.dgt_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class DelaunayBatch(DelaunayGPU):
+    """Many independent periodic sets triangulated / repaired by the same launches.
+    Points of all sets are concatenated; rings hold global point indices."""
+
+    def __init__(self, sizes, boxes, maximumNeighborsGuess: int = 16, cellSizeRelative: float = 1.0):
+        super().__init__(0, maximumNeighborsGuess, 0.0, None, _batch=(list(sizes), list(boxes), cellSizeRelative))
+        self.sizes = [int(s) for s in sizes]
+        self.boxes = [(float(b[0]), float(b[1])) for b in boxes]

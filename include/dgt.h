@@ -1,0 +1,125 @@
+/*
+ * dgt.h -- C ABI of the B200 periodic Delaunay one-ring library (libdgt.so).
+ *
+ * Drop-in boundary for the hot path of the reference class DelaunayGPU
+ * (src/model/DelaunayGPU.h:18-130): per-point construction of the Delaunay one-ring in a
+ * periodic box, and test-and-repair of an existing triangulation.  Plain pointers and sizes
+ * only; every call returns a status code, no exception crosses this boundary.
+ *
+ * Output layout (same as the reference, DelaunayGPU.cpp:47 Index2D(MaxSize, N)):
+ *   tri[i*stride + k], k < neighnum[i]: indices of the Delaunay neighbours of point i in
+ *   counter-clockwise order; rows start at the smallest neighbour index.
+ * Points: double2[n] as 2n doubles (x0,y0,x1,y1,...), every coordinate in [0, L) of its box.
+ * All pointers named d_* are device pointers on the context's device; `stream` is a
+ * cudaStream_t (NULL = legacy default stream).
+ * Contexts are not thread-safe (like the reference class); use one per host thread.
+ */
+#ifndef DGT_H
+#define DGT_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DGT_OK 0
+#define DGT_ERR_INVALID_ARGUMENT 1
+#define DGT_ERR_CUDA 2
+#define DGT_ERR_NEED_RESIZE 3   /* a ring is longer than the row stride; see dgt_get_max_size */
+#define DGT_ERR_DEGENERATE 4    /* a ring could not be closed (duplicate/collinear input) */
+#define DGT_ERR_OUT_OF_MEMORY 5
+#define DGT_ERR_BAD_POINTS 6    /* a coordinate outside [0, L) or not finite */
+#define DGT_ERR_NOT_CONVERGED 7
+
+#define DGT_PRECISION_FP32_FILTER 0 /* float32 filter, float64 recheck, exact residue (default) */
+#define DGT_PRECISION_FP64 1        /* float64 predicates, exact residue */
+
+typedef struct dgt_context dgt_context;
+
+/* counters of the last triangulation / test-and-repair call */
+typedef struct dgt_stats {
+    long long points;          /* ring constructions (build: n; repair: rebuilt points) */
+    long long candidates;      /* candidate points examined */
+    long long tests;           /* circle tests evaluated by the filter stage */
+    long long fp32_undecided;  /* tests the float32 filter left open (re-run in float64) */
+    long long fp64_undecided;  /* tests float64 left open (resolved by exact arithmetic) */
+    long long exact_points;    /* points re-run on the exact / large-ring path */
+    long long mismatches;      /* check mode: filter decisions contradicted by float64 */
+    long long insertions;      /* ring insertions */
+    long long flagged;         /* test-and-repair: points flagged by the local test */
+    long long repaired;        /* test-and-repair: points rebuilt (all rounds) */
+    int repair_rounds;         /* test-and-repair: rounds until no ring changed */
+    int max_ring;              /* largest ring of the call */
+    int error_flags;
+    int reserved;
+} dgt_stats;
+
+/* DelaunayGPU(int N, int maximumNeighborsGuess, double cellSize, PeriodicBoxPtr bx)
+ * (src/model/DelaunayGPU.h:25, DelaunayGPU.cpp:11-37).  Rectangular periodic box Lx x Ly.
+ * cell_size <= 0 picks the cell edge automatically (the mean point spacing). */
+int dgt_create(int n, int max_neighs, double cell_size, double Lx, double Ly, dgt_context **out);
+
+/* Many independent periodic sets in one context: set s has sizes[s] points (concatenated
+ * in set order) and box boxes[2s] x boxes[2s+1].  Rings hold global point indices.
+ * cell_size is relative to each set's mean spacing (<= 0: automatic).  No reference
+ * counterpart: the reference triangulates one set per DelaunayGPU object. */
+int dgt_create_batch(int num_sets, const int *sizes, const double *boxes, double cell_size, int max_neighs,
+                     dgt_context **out);
+
+void dgt_destroy(dgt_context *ctx);
+
+/* globalDelaunayTriangulation(points, GPUTriangulation, cellNeighborNum)
+ * (DelaunayGPU.h:30, DelaunayGPU.cpp:118-157).  d_tri holds n*stride ints.
+ * Returns DGT_ERR_NEED_RESIZE when some ring is longer than stride; dgt_get_max_size then
+ * reports the stride needed (the reference grows its own array, DelaunayGPU.cpp:137-156). */
+int dgt_global_triangulation(dgt_context *ctx, const double *d_points, int *d_tri, int *d_neighnum, int stride,
+                             void *stream);
+
+/* testAndRepairDelaunayTriangulation(points, GPUTriangulation, cellNeighborNum)
+ * (DelaunayGPU.h:33, DelaunayGPU.cpp:567-602): (d_tri, d_neighnum) must hold a valid
+ * triangulation of earlier positions; afterwards they hold the Delaunay triangulation of
+ * d_points.  Only rings that changed are rewritten. */
+int dgt_test_and_repair(dgt_context *ctx, const double *d_points, int *d_tri, int *d_neighnum, int stride,
+                        void *stream);
+
+/* updateList(points) (DelaunayGPU.h:42): rebuild only the cell grid of d_points. */
+int dgt_update_list(dgt_context *ctx, const double *d_points, void *stream);
+
+/* setCellListSize(csize) (DelaunayGPU.h:40) */
+int dgt_set_cell_size(dgt_context *ctx, double cell_size);
+/* setBox(bx) (DelaunayGPU.h:44); single-set contexts only */
+int dgt_set_box(dgt_context *ctx, double Lx, double Ly);
+/* setSafetyMode(sm) (DelaunayGPU.h:46).  On: each call synchronises and reports
+ * DGT_ERR_NEED_RESIZE.  Off: calls return without synchronising; overflowing rings are
+ * written with neighnum 0 and show in dgt_get_stats (never silently truncated). */
+int dgt_set_safety_mode(dgt_context *ctx, int on);
+/* DGT_PRECISION_* */
+int dgt_set_precision(dgt_context *ctx, int precision);
+/* 1: additionally evaluate every float32 decision in float64 and count contradictions */
+int dgt_set_check_mode(dgt_context *ctx, int on);
+/* resize(nmax) (DelaunayGPU.h:38): the ring capacity MaxSize callers should allocate */
+int dgt_resize(dgt_context *ctx, int max_neighs);
+/* MaxSize (DelaunayGPU.h:56): after DGT_ERR_NEED_RESIZE, the stride required */
+int dgt_get_max_size(const dgt_context *ctx, int *out);
+int dgt_get_num_points(const dgt_context *ctx, int *out);
+
+/* Copy rows into an array of another stride (rows keep their neighbours; unused slots 0).
+ * Needed when growing MaxSize of an existing triangulation before a repair. */
+int dgt_restride(const int *d_src, int src_stride, int *d_dst, int dst_stride, const int *d_neighnum, int n,
+                 void *stream);
+
+/* Counters of the last call (synchronises the context's last stream). */
+int dgt_get_stats(dgt_context *ctx, dgt_stats *out);
+
+/* MD-like helper: every point += sigma * N(0,1) per axis (counter-based normals of
+ * (seed, step, index)), wrapped into its box (periodicBoundaries::move,
+ * periodicBoundaries.h:181-189). */
+int dgt_displace(dgt_context *ctx, double *d_points, double sigma, unsigned long long seed, unsigned long long step,
+                 void *stream);
+
+const char *dgt_error_string(int code);
+int dgt_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DGT_H */

@@ -1,0 +1,286 @@
+"""ctypes front end of the CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline / reference legs import
+this module.  It wraps
+
+- ``oracle/liboracle.so`` (``dgt_oracle.c``): a C restatement of the reference's CPU path
+  (src/model/DelaunayGPU.cu:318-608, :680-943, :192-284; src/model/DelaunayGPU.cpp:118-157,
+  :567-602, :673-705; src/utilities/cellListGPU.cpp:97-117, :289-330) and an independent
+  exact-arithmetic Delaunay verifier;
+- ``oracle/_ref/libdgtref.so`` (``ref_harness.cu`` linked with the reference's own sources):
+  the reference itself, run through its CPU/OpenMP callers (no device needed) or through its
+  public ``DelaunayGPU`` class (needs a device).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_PATH = os.path.join(HERE, "_ref", "libdgtref.so")
+
+_P_D = ctypes.POINTER(ctypes.c_double)
+_P_I = ctypes.POINTER(ctypes.c_int)
+
+
+class OrcReport(ctypes.Structure):
+    _fields_ = [
+        ("sum_deg", ctypes.c_longlong),
+        ("bad_index", ctypes.c_longlong),
+        ("asym", ctypes.c_longlong),
+        ("nonpositive", ctypes.c_longlong),
+        ("winding", ctypes.c_longlong),
+        ("not_local_dt", ctypes.c_longlong),
+        ("circle_intruders", ctypes.c_longlong),
+        ("triangles", ctypes.c_longlong),
+        ("min_deg", ctypes.c_int),
+        ("max_deg", ctypes.c_int),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def build(force: bool = False) -> str:
+    """Compile liboracle.so with the Makefile next to this file (gcc; seconds)."""
+    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(
+        os.path.join(HERE, "dgt_oracle.c")
+    ):
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def build_ref() -> str | None:
+    """Compile oracle/_ref/libdgtref.so from the reference's sources when they are present."""
+    if not os.path.isdir(os.environ.get("DGT_REFERENCE_DIR", "/root/reference")):
+        return REF_PATH if os.path.exists(REF_PATH) else None
+    harness = os.path.join(HERE, "ref_harness.cu")
+    if not os.path.exists(REF_PATH) or os.path.getmtime(REF_PATH) < os.path.getmtime(harness):
+        subprocess.run(["bash", os.path.join(HERE, "build_ref.sh")], check=True, capture_output=True)
+    return REF_PATH
+
+
+_lib = None
+_ref = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(LIB_PATH)
+        L.orc_ref_global.restype = ctypes.c_int
+        L.orc_ref_global.argtypes = [_P_D, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_int, ctypes.c_int, _P_I, _P_I]
+        L.orc_ref_test_and_repair.restype = ctypes.c_int
+        L.orc_ref_test_and_repair.argtypes = [_P_D, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                              ctypes.c_double, ctypes.c_int, ctypes.c_int, _P_I, _P_I, _P_I]
+        L.orc_verify.restype = ctypes.c_int
+        L.orc_verify.argtypes = [_P_D, ctypes.c_int, ctypes.c_double, ctypes.c_double, _P_I, _P_I, ctypes.c_int,
+                                 ctypes.c_int, ctypes.c_int, ctypes.POINTER(OrcReport)]
+        L.orc_incircle0.restype = ctypes.c_int
+        L.orc_incircle0.argtypes = [_P_D, _P_D, _P_D]
+        L.orc_orient0.restype = ctypes.c_int
+        L.orc_orient0.argtypes = [_P_D, _P_D]
+        L.orc_offset.restype = None
+        L.orc_offset.argtypes = [_P_D, _P_D, ctypes.c_double, ctypes.c_double, _P_D]
+        L.orc_canonical_rotate.restype = None
+        L.orc_canonical_rotate.argtypes = [_P_I, _P_I, ctypes.c_int, ctypes.c_int]
+        _lib = L
+    return _lib
+
+
+def ref_lib():
+    """The reference itself (oracle/_ref), or None when it was not built."""
+    global _ref
+    if _ref is None:
+        path = build_ref()
+        if path is None or not os.path.exists(path):
+            return None
+        R = ctypes.CDLL(path)
+        R.ref_fn_global.restype = ctypes.c_int
+        R.ref_fn_global.argtypes = [_P_D, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_int, ctypes.c_int, _P_I, _P_I]
+        R.ref_fn_test_and_repair.restype = ctypes.c_int
+        R.ref_fn_test_and_repair.argtypes = [_P_D, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                             ctypes.c_double, ctypes.c_int, ctypes.c_int, _P_I, _P_I, _P_I]
+        R.ref_cls_create.restype = ctypes.c_void_p
+        R.ref_cls_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_double, ctypes.c_int]
+        R.ref_cls_global.restype = ctypes.c_int
+        R.ref_cls_global.argtypes = [ctypes.c_void_p, _P_D, _P_I, _P_I, ctypes.c_int]
+        R.ref_cls_test_and_repair.restype = ctypes.c_int
+        R.ref_cls_test_and_repair.argtypes = [ctypes.c_void_p, _P_D, _P_I, _P_I, ctypes.c_int]
+        R.ref_cls_destroy.restype = None
+        R.ref_cls_destroy.argtypes = [ctypes.c_void_p]
+        R.ref_omp_max_threads.restype = ctypes.c_int
+        _ref = R
+    return _ref
+
+
+def _pd(a):
+    return a.ctypes.data_as(_P_D)
+
+
+def _pi(a):
+    return a.ctypes.data_as(_P_I)
+
+
+@dataclass
+class Triangulation:
+    tri: np.ndarray  # (n, stride) int32, rows hold the CCW ring in their first nn[i] entries
+    nn: np.ndarray   # (n,) int32
+    max_ring: int
+
+    @property
+    def stride(self) -> int:
+        return self.tri.shape[1]
+
+
+def _prep(points):
+    pts = np.ascontiguousarray(points, dtype=np.float64)
+    assert pts.ndim == 2 and pts.shape[1] == 2
+    return pts
+
+
+def default_threads() -> int:
+    return max(1, os.cpu_count() or 1)
+
+
+def restated_global(points, Lx, Ly, cell_size=1.0, stride=32, threads=None) -> Triangulation:
+    """The C restatement of the reference's global triangulation (host path)."""
+    pts = _prep(points)
+    n = len(pts)
+    tri = np.zeros((n, stride), np.int32)
+    nn = np.zeros(n, np.int32)
+    r = lib().orc_ref_global(_pd(pts), n, Lx, Ly, cell_size, stride, threads or default_threads(), _pi(tri), _pi(nn))
+    if r < 0:
+        raise RuntimeError(f"restated global triangulation failed ({r})")
+    return Triangulation(tri, nn, r)
+
+
+def restated_test_and_repair(points, Lx, Ly, tri: Triangulation, cell_size=1.0, threads=None):
+    """The C restatement of the reference's test-and-repair, on a copy of ``tri``.
+    Returns (Triangulation, repair flags)."""
+    pts = _prep(points)
+    n = len(pts)
+    t = np.ascontiguousarray(tri.tri.copy())
+    nn = np.ascontiguousarray(tri.nn.copy())
+    rep = np.zeros(n, np.int32)
+    r = lib().orc_ref_test_and_repair(_pd(pts), n, Lx, Ly, cell_size, t.shape[1], threads or default_threads(),
+                                      _pi(t), _pi(nn), _pi(rep))
+    if r < 0:
+        raise RuntimeError(f"restated test-and-repair failed ({r})")
+    return Triangulation(t, nn, int(nn.max())), rep
+
+
+def reference_global(points, Lx, Ly, cell_size=1.0, stride=32, threads=None) -> Triangulation:
+    """The reference's own host path (oracle/_ref, callers with GPUcompute=false)."""
+    R = ref_lib()
+    if R is None:
+        raise RuntimeError("oracle/_ref/libdgtref.so is not built")
+    pts = _prep(points)
+    n = len(pts)
+    tri = np.zeros((n, stride), np.int32)
+    nn = np.zeros(n, np.int32)
+    r = R.ref_fn_global(_pd(pts), n, Lx, Ly, cell_size, stride, threads or default_threads(), _pi(tri), _pi(nn))
+    return Triangulation(tri, nn, r)
+
+
+def reference_test_and_repair(points, Lx, Ly, tri: Triangulation, cell_size=1.0, threads=None):
+    R = ref_lib()
+    if R is None:
+        raise RuntimeError("oracle/_ref/libdgtref.so is not built")
+    pts = _prep(points)
+    n = len(pts)
+    t = np.ascontiguousarray(tri.tri.copy())
+    nn = np.ascontiguousarray(tri.nn.copy())
+    rep = np.zeros(n, np.int32)
+    r = R.ref_fn_test_and_repair(_pd(pts), n, Lx, Ly, cell_size, t.shape[1], threads or default_threads(),
+                                 _pi(t), _pi(nn), _pi(rep))
+    if r < 0:
+        raise RuntimeError(f"reference test-and-repair failed ({r})")
+    return Triangulation(t, nn, int(nn.max())), rep
+
+
+class ReferenceClass:
+    """The reference's public DelaunayGPU class on its host path (needs a CUDA device)."""
+
+    def __init__(self, n, max_neighs, cell_size, Lx, Ly, threads=None):
+        R = ref_lib()
+        if R is None:
+            raise RuntimeError("oracle/_ref/libdgtref.so is not built")
+        self.R = R
+        self.n = n
+        self.h = R.ref_cls_create(n, max_neighs, cell_size, Lx, Ly, threads or default_threads())
+        if not self.h:
+            raise RuntimeError("reference DelaunayGPU construction failed")
+
+    def global_triangulation(self, points, stride=32, fetch=True):
+        pts = _prep(points)
+        tri = np.zeros((self.n, stride), np.int32) if fetch else None
+        nn = np.zeros(self.n, np.int32) if fetch else None
+        r = self.R.ref_cls_global(self.h, _pd(pts), _pi(tri) if fetch else None, _pi(nn) if fetch else None, stride)
+        if r < 0:
+            raise RuntimeError("reference globalDelaunayTriangulation failed")
+        return Triangulation(tri, nn, r) if fetch else None
+
+    def test_and_repair(self, points, stride=32, fetch=True):
+        pts = _prep(points)
+        tri = np.zeros((self.n, stride), np.int32) if fetch else None
+        nn = np.zeros(self.n, np.int32) if fetch else None
+        r = self.R.ref_cls_test_and_repair(self.h, _pd(pts), _pi(tri) if fetch else None,
+                                           _pi(nn) if fetch else None, stride)
+        if r < 0:
+            raise RuntimeError("reference testAndRepairDelaunayTriangulation failed")
+        return Triangulation(tri, nn, r) if fetch else None
+
+    def close(self):
+        if self.h:
+            self.R.ref_cls_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def verify(points, Lx, Ly, tri, nn, global_scan=True, threads=None):
+    """Exact check that (tri, nn) is the Delaunay triangulation.  Returns (ok, report dict)."""
+    pts = _prep(points)
+    t = np.ascontiguousarray(tri, dtype=np.int32)
+    nnv = np.ascontiguousarray(nn, dtype=np.int32)
+    rep = OrcReport()
+    r = lib().orc_verify(_pd(pts), len(pts), Lx, Ly, _pi(t), _pi(nnv), t.shape[1], 1 if global_scan else 0,
+                         threads or default_threads(), ctypes.byref(rep))
+    return r == 0, rep.as_dict()
+
+
+def canonical(tri, nn):
+    """Copy of the rings rotated so each starts at its smallest index; unused slots -> -1."""
+    t = np.ascontiguousarray(np.array(tri, dtype=np.int32, copy=True))
+    nnv = np.ascontiguousarray(nn, dtype=np.int32)
+    lib().orc_canonical_rotate(_pi(t), _pi(nnv), t.shape[0], t.shape[1])
+    cols = np.arange(t.shape[1])[None, :]
+    t[cols >= nnv[:, None]] = -1
+    return t
+
+
+def incircle0(a, b, d) -> int:
+    a = np.ascontiguousarray(a, np.float64)
+    b = np.ascontiguousarray(b, np.float64)
+    d = np.ascontiguousarray(d, np.float64)
+    return lib().orc_incircle0(_pd(a), _pd(b), _pd(d))
+
+
+def orient0(a, b) -> int:
+    a = np.ascontiguousarray(a, np.float64)
+    b = np.ascontiguousarray(b, np.float64)
+    return lib().orc_orient0(_pd(a), _pd(b))

@@ -1,0 +1,68 @@
+"""CPU checks of the drop-in boundary: libdgt.so loads, exports every function include/dgt.h
+declares, rejects bad arguments with status codes (no GPU needed for those), and the C++
+adapter header compiles."""
+import ctypes
+import os
+import re
+import shutil
+import subprocess
+
+import pytest
+
+from gpudelaunaytriangulation_b200 import _native as N
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "dgt.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(dgt_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_loads_and_exports_header():
+    L = N.lib()
+    names = declared_functions()
+    assert names, "no declarations parsed"
+    assert sorted(N.EXPORTED) == names
+    for name in names:
+        assert hasattr(L, name), name
+    out = subprocess.run(["nm", "-D", "--defined-only", N.library_path()], capture_output=True, text=True).stdout
+    for name in names:
+        assert re.search(rf"\bT {name}$", out, re.M), name
+
+
+def test_error_strings_and_version():
+    L = N.lib()
+    assert L.dgt_version() >= 1
+    for code in range(8):
+        assert L.dgt_error_string(code)
+    assert b"unknown" in L.dgt_error_string(99)
+
+
+def test_invalid_arguments_without_device():
+    L = N.lib()
+    h = ctypes.c_void_p()
+    assert L.dgt_create(-1, 16, 1.0, 10.0, 10.0, ctypes.byref(h)) == N.DGT_ERR_INVALID_ARGUMENT
+    assert L.dgt_create(10, 16, 1.0, 0.0, 10.0, ctypes.byref(h)) == N.DGT_ERR_INVALID_ARGUMENT
+    assert L.dgt_create(10, 16, float("nan"), 10.0, 10.0, ctypes.byref(h)) == N.DGT_ERR_INVALID_ARGUMENT
+    assert L.dgt_create(10, 16, 1.0, 10.0, 10.0, None) == N.DGT_ERR_INVALID_ARGUMENT
+    assert L.dgt_create_batch(0, None, None, 1.0, 16, ctypes.byref(h)) == N.DGT_ERR_INVALID_ARGUMENT
+    assert L.dgt_global_triangulation(None, None, None, None, 16, None) == N.DGT_ERR_INVALID_ARGUMENT
+    assert L.dgt_test_and_repair(None, None, None, None, 16, None) == N.DGT_ERR_INVALID_ARGUMENT
+    assert L.dgt_set_precision(None, 0) == N.DGT_ERR_INVALID_ARGUMENT
+    v = ctypes.c_int()
+    assert L.dgt_get_max_size(None, ctypes.byref(v)) == N.DGT_ERR_INVALID_ARGUMENT
+    assert L.dgt_restride(None, 4, None, 8, None, 5, None) == N.DGT_ERR_INVALID_ARGUMENT
+    L.dgt_destroy(None)
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="no host C++ compiler")
+def test_cpp_adapter_header_compiles(tmp_path):
+    src = tmp_path / "use.cpp"
+    src.write_text('#include "dgt_delaunay.hpp"\nint main(){ return 0; }\n')
+    cuda_inc = "/usr/local/cuda/include"
+    r = subprocess.run(["g++", "-std=c++14", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), "-I", cuda_inc,
+                        str(src)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr

@@ -1,0 +1,277 @@
+"""GPU parity: the CUDA path (through the C ABI) against the oracle.
+
+Bar: rings bit-identical after canonical rotation to the reference's own output (golden
+fixtures made from oracle/_ref) and to the C restatement of the reference, every
+triangulation accepted by the exact verifier (consistent rings, CCW fans winding once,
+every edge locally Delaunay, every circumcircle empty, sum of ring sizes = 6N), and zero
+float32-filter decisions contradicted by float64 in check mode."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from gpudelaunaytriangulation_b200 import workloads as W
+from oracle import oracle as O
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+
+
+def _dg():
+    from gpudelaunaytriangulation_b200.delaunay import DelaunayGPU
+
+    return DelaunayGPU
+
+
+def flat(tri, nn):
+    c = O.canonical(tri, nn)
+    return np.concatenate([c[i, : nn[i]] for i in range(len(nn))]).astype(np.int32)
+
+
+def gpu_build(pts, Lx, Ly, cell=1.0, maxn=16, fp32=True, check=False):
+    n = len(pts)
+    d = _dg()(n, maxn, cell, (Lx, Ly))
+    d.setPrecision(fp32)
+    d.setCheckMode(check)
+    P = torch.from_numpy(np.ascontiguousarray(pts)).cuda()
+    tri, nn = d.globalDelaunayTriangulation(P)
+    torch.cuda.synchronize()
+    return d, P, tri, nn
+
+
+def host(tri, nn):
+    n = nn.numel()
+    return tri.view(n, -1).cpu().numpy(), nn.cpu().numpy()
+
+
+def assert_delaunay(pts, Lx, Ly, t, nn, scan=True):
+    ok, rep = O.verify(pts, Lx, Ly, t, nn, global_scan=scan)
+    assert ok, rep
+    assert rep["sum_deg"] == 6 * len(pts)
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+@pytest.mark.parametrize("fp32", [True, False], ids=["fp32filter", "fp64"])
+def test_build_matches_reference_golden(path, fp32):
+    g = np.load(path)
+    L = g["L"]
+    d, P, tri, nn = gpu_build(g["points"], L[0], L[1], float(g["cell_size"]), 16, fp32, check=True)
+    t, k = host(tri, nn)
+    assert np.array_equal(k, g["nn"])
+    assert np.array_equal(flat(t, k), g["rings"])
+    st = d.stats()
+    assert st["mismatches"] == 0 and st["error_flags"] == 0
+    assert_delaunay(g["points"], L[0], L[1], t, k)
+
+
+@pytest.mark.parametrize("path", [p for p in GOLDEN if "n10000" not in p], ids=lambda p: os.path.basename(p))
+def test_repair_matches_reference_golden(path):
+    g = np.load(path)
+    L = g["L"]
+    d, P, tri, nn = gpu_build(g["points"], L[0], L[1], float(g["cell_size"]))
+    P.copy_(torch.from_numpy(g["moved"]))
+    d.testAndRepairDelaunayTriangulation(P, tri, nn)
+    t, k = host(tri, nn)
+    assert np.array_equal(k, g["repair_nn"])
+    assert np.array_equal(flat(t, k), g["repair_rings"])
+
+
+@pytest.mark.parametrize("n,seed,cell", [(1000, 31, 1.0), (50000, 32, 1.0), (50000, 33, 0.6), (50000, 34, 2.0)])
+def test_build_matches_restated_reference(n, seed, cell):
+    L = float(np.sqrt(n))
+    pts = W.uniform_points(n, L, seed)
+    ref = O.restated_global(pts, L, L, 1.0, 32)
+    for fp32 in (True, False):
+        d, P, tri, nn = gpu_build(pts, L, L, cell, 16, fp32, check=True)
+        t, k = host(tri, nn)
+        assert np.array_equal(k, ref.nn)
+        assert np.array_equal(O.canonical(t, k)[:, :16], O.canonical(ref.tri, ref.nn)[:, :16])
+        st = d.stats()
+        assert st["mismatches"] == 0, st
+        assert st["points"] + st["exact_points"] >= n
+
+
+def test_fp32_filter_and_fp64_identical_and_counted():
+    n = 200000
+    L = float(np.sqrt(n))
+    pts = W.uniform_points(n, L, 41)
+    d1, _, t1, k1 = gpu_build(pts, L, L, 1.0, 16, True, check=True)
+    s1 = d1.stats()
+    d2, _, t2, k2 = gpu_build(pts, L, L, 1.0, 16, False)
+    assert torch.equal(k1, k2) and torch.equal(t1, t2)
+    assert s1["mismatches"] == 0
+    assert s1["tests"] > 0 and s1["fp32_undecided"] < 1e-3 * s1["tests"]
+    t, k = host(t1, k1)
+    assert_delaunay(pts, L, L, t, k, scan=False)
+
+
+@pytest.mark.parametrize("sigma,steps", [(0.02, 4), (0.1, 2)])
+def test_repair_steps_match_fresh_triangulation(sigma, steps):
+    n = 30000
+    L = float(np.sqrt(n))
+    pts = W.uniform_points(n, L, 51)
+    d, P, tri, nn = gpu_build(pts, L, L)
+    cur = pts
+    for s in range(steps):
+        cur = W.displace(cur, sigma, L, L, 900 + s)
+        P.copy_(torch.from_numpy(cur))
+        d.testAndRepairDelaunayTriangulation(P, tri, nn)
+        t, k = host(tri, nn)
+        ref = O.restated_global(cur, L, L, 1.0, 32)
+        assert np.array_equal(k, ref.nn)
+        assert np.array_equal(O.canonical(t, k)[:, :16], O.canonical(ref.tri, ref.nn)[:, :16])
+        st = d.stats()
+        assert st["flagged"] > 0 and st["repair_rounds"] >= 1 and st["error_flags"] == 0
+
+
+def test_repair_of_reference_style_local_moves():
+    # triangulation.cpp:322-364: a random 5% of points each moved by U(-0.1, 0.1) per axis
+    n = 20000
+    L = float(np.sqrt(n))
+    pts = W.uniform_points(n, L, 61)
+    d, P, tri, nn = gpu_build(pts, L, L)
+    rng = np.random.default_rng(61)
+    idx = rng.permutation(n)[: n // 20]
+    moved = pts.copy()
+    moved[idx] += rng.uniform(-0.1, 0.1, size=(len(idx), 2))
+    moved = W.wrap(moved, L, L)
+    P.copy_(torch.from_numpy(moved))
+    d.testAndRepairDelaunayTriangulation(P, tri, nn)
+    t, k = host(tri, nn)
+    ref = O.restated_global(moved, L, L, 1.0, 32)
+    assert np.array_equal(O.canonical(t, k)[:, :16], O.canonical(ref.tri, ref.nn)[:, :16])
+    assert d.stats()["repaired"] < n // 2
+
+
+def test_gpu_displacement_then_repair():
+    n = 40000
+    L = float(np.sqrt(n))
+    pts = W.uniform_points(n, L, 71)
+    d, P, tri, nn = gpu_build(pts, L, L)
+    for step in range(3):
+        d.displace(P, 0.02, seed=7, step=step)
+        d.testAndRepairDelaunayTriangulation(P, tri, nn)
+    cur = P.cpu().numpy()
+    assert (cur >= 0).all() and (cur < L).all()
+    t, k = host(tri, nn)
+    ref = O.restated_global(cur, L, L, 1.0, 32)
+    assert np.array_equal(O.canonical(t, k)[:, :16], O.canonical(ref.tri, ref.nn)[:, :16])
+
+
+@pytest.mark.parametrize("n", [12, 40, 100, 333])
+def test_small_sets(n):
+    L = float(np.sqrt(n))
+    pts = W.uniform_points(n, L, 81 + n)
+    d, P, tri, nn = gpu_build(pts, L, L, 1.0, 16)
+    t, k = host(tri, nn)
+    ref = O.restated_global(pts, L, L, 1.0, 32)
+    assert np.array_equal(O.canonical(t, k)[:, :16], O.canonical(ref.tri, ref.nn)[:, :16])
+
+
+def test_rectangular_lattice_box():
+    pts, Lx, Ly = W.triangular_lattice(64, 64, 1.0, 1e-4, seed=3)
+    for fp32 in (True, False):
+        d, P, tri, nn = gpu_build(pts, Lx, Ly, 0.0, 16, fp32, check=True)
+        t, k = host(tri, nn)
+        assert (k == 6).all()
+        assert_delaunay(pts, Lx, Ly, t, k)
+        assert d.stats()["mismatches"] == 0
+
+
+def test_clustered_gaussian_mixture():
+    pts, L = W.gaussian_mixture(40000, components=16, sigma=2.0, seed=9)
+    d, P, tri, nn = gpu_build(pts, L, L, 0.0, 16, True, check=True)
+    t, k = host(tri, nn)
+    assert_delaunay(pts, L, L, t, k)
+    ref = O.restated_global(pts, L, L, 1.0, 48)
+    assert np.array_equal(O.canonical(t, k)[:, : t.shape[1]], O.canonical(ref.tri, ref.nn)[:, : t.shape[1]])
+
+
+def test_safety_mode_grows_stride():
+    n = 5000
+    L = float(np.sqrt(n))
+    pts = W.uniform_points(n, L, 91)
+    d, P, tri, nn = gpu_build(pts, L, L, 1.0, 4)   # 4 slots: every point overflows first
+    t, k = host(tri, nn)
+    assert d.MaxSize == int(k.max()) and t.shape[1] == d.MaxSize
+    assert_delaunay(pts, L, L, t, k)
+
+
+def test_no_safety_mode_raises_instead_of_truncating():
+    from gpudelaunaytriangulation_b200 import _native as N
+
+    n = 5000
+    L = float(np.sqrt(n))
+    pts = W.uniform_points(n, L, 92)
+    d = _dg()(n, 5, 1.0, (L, L))
+    P = torch.from_numpy(pts).cuda()
+    tri = torch.zeros(5 * n, dtype=torch.int32, device="cuda")
+    nn = torch.zeros(n, dtype=torch.int32, device="cuda")
+    d.safetyMode = False   # python-side growth off, library still reports
+    with pytest.raises(N.DgtError) as e:
+        d.globalDelaunayTriangulation(P, tri, nn)
+    assert e.value.code == N.DGT_ERR_NEED_RESIZE
+    assert d.MaxSize > 5
+
+
+def test_bad_points_rejected():
+    from gpudelaunaytriangulation_b200 import _native as N
+
+    n = 1000
+    L = float(np.sqrt(n))
+    pts = W.uniform_points(n, L, 93)
+    pts[5, 0] = L   # outside [0, L)
+    with pytest.raises(N.DgtError) as e:
+        gpu_build(pts, L, L)
+    assert e.value.code == N.DGT_ERR_BAD_POINTS
+
+
+def test_batched_sets_match_per_set_oracle():
+    from gpudelaunaytriangulation_b200.delaunay import DelaunayBatch
+
+    pts, sizes, boxes = W.ensemble(12, 200, 5000, seed=13)
+    b = DelaunayBatch(sizes, boxes, 16, 1.0)
+    b.setCheckMode(True)
+    P = torch.from_numpy(pts).cuda()
+    tri, nn = b.globalDelaunayTriangulation(P)
+    t, k = host(tri, nn)
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    for s in range(len(sizes)):
+        lo, hi = off[s], off[s + 1]
+        ref = O.restated_global(pts[lo:hi], boxes[s][0], boxes[s][1], 1.0, 32)
+        ts = t[lo:hi].copy()
+        ts[np.arange(ts.shape[1])[None, :] < k[lo:hi, None]] -= lo
+        assert np.array_equal(k[lo:hi], ref.nn)
+        assert np.array_equal(O.canonical(ts, k[lo:hi])[:, :16], O.canonical(ref.tri, ref.nn)[:, :16])
+    assert b.stats()["mismatches"] == 0
+    # batched repair after a displacement of every set
+    for step in range(2):
+        b.displace(P, 0.01, seed=3, step=step)
+        b.testAndRepairDelaunayTriangulation(P, tri, nn)
+    cur = P.cpu().numpy()
+    t, k = host(tri, nn)
+    for s in range(len(sizes)):
+        lo, hi = off[s], off[s + 1]
+        ref = O.restated_global(cur[lo:hi], boxes[s][0], boxes[s][1], 1.0, 32)
+        ts = t[lo:hi].copy()
+        ts[np.arange(ts.shape[1])[None, :] < k[lo:hi, None]] -= lo
+        assert np.array_equal(O.canonical(ts, k[lo:hi])[:, :16], O.canonical(ref.tri, ref.nn)[:, :16])
+
+
+def test_million_points_properties():
+    n = 1_000_000
+    L = 1000.0
+    pts = W.uniform_points(n, L, 101)
+    d, P, tri, nn = gpu_build(pts, L, L, 1.0, 16)
+    t, k = host(tri, nn)
+    assert int(k.sum()) == 6 * n
+    assert_delaunay(pts, L, L, t, k, scan=False)
+    moved = W.displace(pts, 0.02, L, L, 102)
+    P.copy_(torch.from_numpy(moved))
+    d.testAndRepairDelaunayTriangulation(P, tri, nn)
+    t, k = host(tri, nn)
+    assert int(k.sum()) == 6 * n
+    assert_delaunay(moved, L, L, t, k, scan=False)
