@@ -1,0 +1,418 @@
+#!/usr/bin/env python
+"""Benchmark of the periodic Delaunay hot path: full triangulation + one test-and-repair step.
+
+Workload (default "build_repair_4m"): N = 4,194,304 i.i.d. uniform points in a periodic
+square of side L = 2048 (unit density), float64 coordinates, cell size 1.0.  One step is
+  globalDelaunayTriangulation(P0) -> testAndRepairDelaunayTriangulation(P1)
+with P1 = P0 displaced by N(0, 0.02^2) per axis and wrapped (displacement precomputed, as in
+an MD code that hands the new positions over).  Predicates: float32 filter -> float64 ->
+exact (the "fp64_plain" key repeats the measurement with float64 predicates).
+Metric: Mpoints/s = N / step time (each point goes through one build and one repair).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Under torchrun each rank runs an independent replica (no data-path collective: the sets
+are independent); value = all ranks' points / max-over-ranks device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+from gpudelaunaytriangulation_b200 import workloads as W  # noqa: E402
+
+METRIC = "Mpoints/s full build + repair on 1 B200, FP32-filter vs FP64 plain, 0 mismatches"
+UNIT = "Mpoints/s"
+
+WORKLOADS = {
+    # name: (n, L, sigma, cell size, maxNeighs)
+    "build_repair_4m": (4_194_304, 2048.0, 0.02, 1.0, 16),
+    "build_repair_1m": (1_000_000, 1000.0, 0.02, 1.0, 16),
+}
+
+# Algorithmic (compulsory) DRAM bytes per point of the one-ring kernel k_build: own position
+# (16 B) + own index (4 B) + cell start (4 B) + ring written (6 neighbours x 4 B on average,
+# exactly 6 on the torus) + ring length (4 B).  Candidate re-reads served on chip are not
+# counted.
+BUILD_BYTES_PER_POINT = 16 + 4 + 4 + 24 + 4
+# DRAM bytes per point that ncu measured for k_build (dram__bytes_read.sum +
+# dram__bytes_write.sum over one launch / points), profiles/k_build_fp32_4m.md; None until
+# a capture exists.
+BUILD_DRAM_BYTES_PER_POINT_NCU = None
+FALLBACK_HBM_GBS = 6650.0
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+class _StdoutToStderr:
+    """The reference library prints progress with printf; keep fd 1 for the JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        return False
+
+
+def reference_cpu_run(n, L, sigma, cell, maxn, steps, warmup, seed, threads=None, budget_s=None):
+    with _StdoutToStderr():
+        return _reference_cpu_run(n, L, sigma, cell, maxn, steps, warmup, seed, threads, budget_s)
+
+
+def _reference_cpu_run(n, L, sigma, cell, maxn, steps, warmup, seed, threads=None, budget_s=None):
+    """The reference's own host path (oracle/_ref: DelaunayGPU class, GPUcompute=false,
+    OpenMP over all host threads), build + test-and-repair per step.  Falls back to the C
+    restatement (oracle/liboracle.so) when the reference library is absent."""
+    from oracle import oracle as O
+
+    threads = threads or O.default_threads()
+    p0 = W.uniform_points(n, L, seed)
+    p1 = W.displace(p0, sigma, L, L, seed + 1)
+    kind = "reference"
+    cls = None
+    try:
+        if O.ref_lib() is None:
+            raise RuntimeError("oracle/_ref not built")
+        cls = O.ReferenceClass(n, max(maxn, 24), cell, L, L, threads)
+    except Exception:
+        kind = "port"
+    times = []
+    total = warmup + steps
+    t_start = time.perf_counter()
+    for it in range(total):
+        t0 = time.perf_counter()
+        if cls is not None:
+            cls.global_triangulation(p0, fetch=False)
+            cls.test_and_repair(p1, fetch=False)
+        else:
+            t = O.restated_global(p0, L, L, cell, 32, threads)
+            O.restated_test_and_repair(p1, L, L, t, cell, threads)
+        dt = time.perf_counter() - t0
+        if it >= warmup:
+            times.append(dt)
+        if budget_s is not None and time.perf_counter() - t_start > budget_s and len(times) >= 1:
+            break
+    if cls is not None:
+        cls.close()
+    return {"seconds": times, "kind": kind, "threads": threads}
+
+
+def run_reference(args):
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return 0
+    n, L, sigma, cell, maxn = WORKLOADS[args.workload]
+    if args.n:
+        n, L = args.n, float(np.sqrt(args.n))
+    r = reference_cpu_run(n, L, sigma, cell, maxn, args.steps, args.warmup, seed=2026)
+    secs = r["seconds"]
+    mean = sum(secs) / len(secs)
+    value = n / mean / 1e6
+    out = {
+        "impl": "reference",
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": len(secs),
+        "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded uniform periodic points)",
+        "config": {"workload": args.workload, "n_points": n, "box": L, "sigma": sigma, "cell_size": cell,
+                   "path": "reference DelaunayGPU host path (GPUcompute=false, OpenMP)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": r["threads"], "kind": r["kind"],
+                         "sample": f"full workload: build + one repair of {n} points per step",
+                         "cpu": cpu_model()},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from gpudelaunaytriangulation_b200.delaunay import DelaunayGPU
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    n, L, sigma, cell, maxn = WORKLOADS[args.workload]
+    if args.n:
+        n, L = args.n, float(np.sqrt(args.n))
+    seed = 2026 + 7919 * rank
+    p0 = W.uniform_points(n, L, seed)
+    p1 = W.displace(p0, sigma, L, L, seed + 1)
+    P0 = torch.from_numpy(p0).to(dev)
+    P1 = torch.from_numpy(p1).to(dev)
+    tri = torch.zeros(maxn * n, dtype=torch.int32, device=dev)
+    nn = torch.zeros(n, dtype=torch.int32, device=dev)
+    d = DelaunayGPU(n, maxn, cell, (L, L))
+    d.setTiming(True)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(precision_fp32: bool, steps: int, warmup: int, sample_clocks=False):
+        d.setPrecision(precision_fp32)
+        for _ in range(warmup):
+            d.globalDelaunayTriangulation(P0, tri, nn)
+            d.testAndRepairDelaunayTriangulation(P1, tri, nn)
+        build_ms, launches, repaired, rounds = [], 0, 0, []
+        clocks = ClockSampler(local) if sample_clocks else None
+        barrier()
+        torch.cuda.synchronize()
+        if clocks:
+            clocks.start()
+            time.sleep(0.3)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            d.globalDelaunayTriangulation(P0, tri, nn)
+            build_ms.append(d.phaseTimes()["build"])
+            launches += d.stats()["launches"]
+            d.testAndRepairDelaunayTriangulation(P1, tri, nn)
+            st = d.stats()
+            launches += st["launches"]
+            repaired += st["repaired"]
+            rounds.append(st["repair_rounds"])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ck = clocks.stop() if clocks else None
+        ms = e0.elapsed_time(e1) / steps
+        return max_over_ranks(ms), build_ms, launches, repaired / steps, rounds, ck
+
+    # headline: float32 filter
+    ms, build_ms, launches, repaired, rounds, clocks = timed(True, args.steps, args.warmup, sample_clocks=True)
+    value = world * n / (ms / 1e3) / 1e6
+    # phase split of one extra step (outside the timed region)
+    d.globalDelaunayTriangulation(P0, tri, nn)
+    ph_build = d.phaseTimes()
+    d.testAndRepairDelaunayTriangulation(P1, tri, nn)
+    ph_rep = d.phaseTimes()
+    st_rep = d.stats()
+    # float64-plain variant, same workload
+    ms64, build_ms64, _, _, _, _ = timed(False, max(2, args.steps // 2), 1)
+    value64 = world * n / (ms64 / 1e3) / 1e6
+    # check mode (outside timing): every float32 decision re-evaluated in float64
+    d.setPrecision(True)
+    d.setCheckMode(True)
+    d.globalDelaunayTriangulation(P0, tri, nn)
+    chk_b = d.stats()
+    d.testAndRepairDelaunayTriangulation(P1, tri, nn)
+    chk_r = d.stats()
+    d.setCheckMode(False)
+
+    # end to end through the public API with host buffers (pinned), copies inside the region
+    e2e = None
+    if not args.no_e2e:
+        h0 = torch.from_numpy(p0).pin_memory()
+        h1 = torch.from_numpy(p1).pin_memory()
+        htri = torch.empty(tri.numel(), dtype=torch.int32).pin_memory()
+        hnn = torch.empty(n, dtype=torch.int32).pin_memory()
+        Pd = torch.empty_like(P0)
+        e_steps = max(2, args.steps // 2)
+
+        def e2e_step():
+            Pd.copy_(h0, non_blocking=True)
+            d.globalDelaunayTriangulation(Pd, tri, nn)
+            htri.copy_(tri, non_blocking=True)
+            hnn.copy_(nn, non_blocking=True)
+            Pd.copy_(h1, non_blocking=True)
+            d.testAndRepairDelaunayTriangulation(Pd, tri, nn)
+            htri.copy_(tri, non_blocking=True)
+            hnn.copy_(nn, non_blocking=True)
+
+        e2e_step()
+        torch.cuda.synchronize()
+        barrier()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(e_steps):
+            e2e_step()
+        f1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ems = max_over_ranks(f0.elapsed_time(f1) / e_steps)
+        e2e = {"value": world * n / (ems / 1e3) / 1e6, "unit": UNIT,
+               "h2d_bytes_per_step": 2 * P0.numel() * 8,
+               "d2h_bytes_per_step": 2 * (tri.numel() + nn.numel()) * 4, "ms_per_step": ems}
+
+    peak, peak_kind = measured_peaks()
+    avg_build_s = (sum(build_ms) / len(build_ms)) / 1e3
+    bytes_launch = n * BUILD_BYTES_PER_POINT
+    achieved = bytes_launch / avg_build_s / 1e9
+    traffic = None if BUILD_DRAM_BYTES_PER_POINT_NCU is None else BUILD_DRAM_BYTES_PER_POINT_NCU * n
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = reference_cpu_run(n, L, sigma, cell, maxn, steps=1, warmup=0, seed=seed, budget_s=30)
+        cpu = {"value": n / (sum(r["seconds"]) / len(r["seconds"])) / 1e6, "unit": UNIT, "cores": r["threads"],
+               "kind": r["kind"], "cpu": cpu_model(),
+               "sample": f"one full step (build + one repair of {n} points) of the same workload"}
+
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded uniform periodic points)",
+        "config": {"workload": args.workload, "n_points": n, "box": L, "sigma": sigma, "cell_size": cell,
+                   "max_neighs": maxn, "precision": "fp32 filter -> fp64 -> exact",
+                   "l2": "working set (positions 64 MB x2 + rings 268 MB) larger than the 126 MB L2",
+                   "parallelism": f"{world} independent replica(s)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "kernel": "k_build<float,14,64> (one-ring construction)",
+                     "bytes_per_point": BUILD_BYTES_PER_POINT, "avg_launch_ms": avg_build_s * 1e3,
+                     "peak_source": f"{peak_kind} hbm_gbs"},
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "clocks": clocks,
+        "fp64_plain": {"value": value64, "unit": UNIT, "ms_per_step": ms64,
+                       "build_kernel_ms": sum(build_ms64) / len(build_ms64)},
+        "phases_ms": {"build_call": ph_build, "repair_call": ph_rep},
+        "repair": {"repaired_per_step": repaired, "rounds": rounds, "flagged": st_rep["flagged"]},
+        "fallback": {"fp32_undecided_frac": chk_b["fp32_undecided"] / max(1, chk_b["tests"]),
+                     "fp64_undecided": chk_b["fp64_undecided"] + chk_r["fp64_undecided"],
+                     "exact_points": chk_b["exact_points"] + chk_r["exact_points"],
+                     "tests": chk_b["tests"] + chk_r["tests"]},
+        "mismatches": chk_b["mismatches"] + chk_r["mismatches"],
+    }
+    if rank == 0:
+        print(json.dumps(out))
+    d.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="build_repair_4m")
+    ap.add_argument("--n", type=int, default=0, help="override the point count (box side sqrt(n))")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

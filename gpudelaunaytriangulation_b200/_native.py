@@ -29,8 +29,10 @@ EXPORTED = [
     "dgt_create", "dgt_create_batch", "dgt_destroy", "dgt_global_triangulation", "dgt_test_and_repair",
     "dgt_update_list", "dgt_set_cell_size", "dgt_set_box", "dgt_set_safety_mode", "dgt_set_precision",
     "dgt_set_check_mode", "dgt_resize", "dgt_get_max_size", "dgt_get_num_points", "dgt_restride",
-    "dgt_get_stats", "dgt_displace", "dgt_error_string", "dgt_version",
+    "dgt_get_stats", "dgt_displace", "dgt_error_string", "dgt_version", "dgt_set_timing",
+    "dgt_get_phase_times",
 ]
+PHASES = ["bin", "build", "slow", "test", "repair"]
 
 
 class Stats(ctypes.Structure):
@@ -45,14 +47,15 @@ class Stats(ctypes.Structure):
         ("insertions", ctypes.c_longlong),
         ("flagged", ctypes.c_longlong),
         ("repaired", ctypes.c_longlong),
+        ("cells", ctypes.c_longlong),
         ("repair_rounds", ctypes.c_int),
         ("max_ring", ctypes.c_int),
         ("error_flags", ctypes.c_int),
-        ("reserved", ctypes.c_int),
+        ("launches", ctypes.c_int),
     ]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class DgtError(RuntimeError):
@@ -70,17 +73,16 @@ def library_path() -> str:
 
 
 def lib() -> ctypes.CDLL:
-    """Load libdgt.so (building it first if the sources are newer and nvcc is available)."""
+    """Load libdgt.so (built in-tree by build.py; built here only if it is missing)."""
     global _lib
     if _lib is not None:
         return _lib
     path = _build.LIB
-    if _build.stale():
+    if not os.path.exists(path):
         try:
             _build.build()
         except Exception as exc:  # pragma: no cover - build failures surface below
-            if not os.path.exists(path):
-                raise RuntimeError(f"libdgt.so is missing and could not be built: {exc}") from exc
+            raise RuntimeError(f"libdgt.so is missing and could not be built: {exc}") from exc
     if not os.path.exists(path):
         raise RuntimeError(f"libdgt.so not found at {path}; run python -m gpudelaunaytriangulation_b200.build")
     L = ctypes.CDLL(path)
@@ -107,6 +109,8 @@ def lib() -> ctypes.CDLL:
     L.dgt_error_string.argtypes = [ctypes.c_int]
     L.dgt_error_string.restype = ctypes.c_char_p
     L.dgt_version.restype = ctypes.c_int
+    L.dgt_set_timing.argtypes = [vp, ctypes.c_int]
+    L.dgt_get_phase_times.argtypes = [vp, P_D]
     _lib = L
     return L
 

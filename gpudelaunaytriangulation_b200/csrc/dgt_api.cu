@@ -49,7 +49,8 @@ struct DevBuf {
 };
 
 constexpr int SLOW_ITEMS = 2048;    // concurrent exact / large-ring items (scratch rows)
-constexpr int ASYNC_ROUNDS = 8;     // repair rounds launched before the first host check
+constexpr int FIRST_ROUNDS = 3;     // repair rounds launched before the first host check
+constexpr int NEXT_ROUNDS = 2;      // rounds per later batch (each kernel exits at once on an empty list)
 
 }  // namespace
 
@@ -74,7 +75,11 @@ struct dgt_context {
     DevStatus *h_st = nullptr;
     cudaStream_t last_stream = nullptr;
     bool stats_valid = false;
-    int pending_rounds_check = 0;   // repair launched without a host check (safety off)
+    int launches = 0;                          // kernels launched by the last call
+    bool timing = false;
+    cudaEvent_t ev[DGT_NUM_PHASES][2] = {};
+    bool ev_used[DGT_NUM_PHASES] = {};
+    int sms = 0;
 };
 
 namespace {
@@ -91,6 +96,43 @@ int cuda_status(cudaError_t e)
         cudaError_t e_ = (expr);                        \
         if (e_ != cudaSuccess) return cuda_status(e_);  \
     } while (0)
+
+struct PhaseTimer {
+    dgt_context *c;
+    int ph;
+    cudaStream_t s;
+    PhaseTimer(dgt_context *cc, int p, cudaStream_t ss) : c(cc), ph(p), s(ss)
+    {
+        if (c->timing) {
+            cudaEventRecord(c->ev[ph][0], s);
+            c->ev_used[ph] = true;
+        }
+    }
+    ~PhaseTimer()
+    {
+        if (c->timing) cudaEventRecord(c->ev[ph][1], s);
+    }
+};
+
+void phase_begin(dgt_context *c, int ph, cudaStream_t s)
+{
+    if (c->timing) {
+        cudaEventRecord(c->ev[ph][0], s);
+        c->ev_used[ph] = true;
+    }
+}
+void phase_end(dgt_context *c, int ph, cudaStream_t s)
+{
+    if (c->timing) cudaEventRecord(c->ev[ph][1], s);
+}
+
+void begin_call(dgt_context *c, cudaStream_t s)
+{
+    c->last_stream = s;
+    c->stats_valid = false;
+    c->launches = 0;
+    for (int p = 0; p < DGT_NUM_PHASES; ++p) c->ev_used[p] = false;
+}
 
 double pow2_at_least(double x)
 {
@@ -179,6 +221,10 @@ int alloc_all(dgt_context *c)
 
 int init_context(dgt_context *c)
 {
+    if (!c->sms) {
+        cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device);
+        if (c->sms <= 0) c->sms = 148;
+    }
     int r = plan_grid(c);
     if (r != DGT_OK) return r;
     return alloc_all(c);
@@ -206,8 +252,10 @@ BinArgs bin_args(dgt_context *c, const double *pts)
 
 cudaError_t run_bin(dgt_context *c, const double *pts, cudaStream_t s)
 {
+    PhaseTimer t(c, DGT_PHASE_BIN, s);
     cudaError_t e = cudaMemsetAsync(c->ccount.p, 0, sizeof(int) * ((size_t)c->total_cells + 1), s);
     if (e != cudaSuccess) return e;
+    c->launches += (c->n > 0 ? 2 : 0) + 3 + (c->deterministic && c->total_cells > 0 ? 1 : 0);
     return launch_bin_st(bin_args(c, pts), c->st.as<DevStatus>(), s);
 }
 
@@ -237,7 +285,14 @@ RingArgs ring_args(dgt_context *c, const double *pts, int *tri, int *nn, int str
 
 cudaError_t run_slow(dgt_context *c, const RingArgs &a, cudaStream_t s)
 {
+    c->launches += 1;
     return launch_slow(a, c->slow_scratch.p, SLOW_ITEMS, 64, s);
+}
+
+cudaError_t run_build(dgt_context *c, const RingArgs &a, cudaStream_t s)
+{
+    c->launches += a.n_items > 0 ? 1 : 0;
+    return launch_build(a, c->precision == DGT_PRECISION_FP64 ? MODE_F64 : MODE_F32, c->sms, s);
 }
 
 void to_stats(const DevStatus &d, dgt_stats *o)
@@ -253,6 +308,7 @@ void to_stats(const DevStatus &d, dgt_stats *o)
     o->insertions = (long long)d.insertions;
     o->flagged = (long long)d.flagged;
     o->repaired = (long long)d.repaired;
+    o->cells = (long long)d.cells;
     o->repair_rounds = d.rounds;
     o->max_ring = d.max_ring;
     o->error_flags = d.err_flags;
@@ -270,7 +326,7 @@ int conclude(dgt_context *c, cudaStream_t s, bool repair_pending)
         c->max_size = std::max(c->max_size, d.need_stride);
         return DGT_ERR_NEED_RESIZE;
     }
-    if (d.err_flags) return DGT_ERR_DEGENERATE;
+    if (d.err_flags & ~EF_MINIMAGE) return DGT_ERR_DEGENERATE;
     if (repair_pending) return DGT_ERR_NOT_CONVERGED;
     return DGT_OK;
 }
@@ -363,6 +419,9 @@ void dgt_destroy(dgt_context *c)
                        &c->slow_scratch, &c->st };
     for (DevBuf *b : bufs) b->release();
     if (c->h_st) cudaFreeHost(c->h_st);
+    for (int p = 0; p < DGT_NUM_PHASES; ++p)
+        for (int k = 0; k < 2; ++k)
+            if (c->ev[p][k]) cudaEventDestroy(c->ev[p][k]);
     delete c;
 }
 
@@ -383,13 +442,18 @@ int dgt_global_triangulation(dgt_context *c, const double *d_points, int *d_tri,
     if (c->n == 0) return DGT_OK;   // DelaunayGPU.cpp:121-125: nothing to do
     if (!d_points || !d_tri || !d_nn || !valid_stride(stride)) return DGT_ERR_INVALID_ARGUMENT;
     cudaStream_t s = (cudaStream_t)stream;
-    c->last_stream = s;
-    c->stats_valid = false;
+    begin_call(c, s);
     DGT_TRY(cudaMemsetAsync(c->st.p, 0, sizeof(DevStatus), s));
     DGT_TRY(run_bin(c, d_points, s));
     RingArgs a = ring_args(c, d_points, d_tri, d_nn, stride);
-    DGT_TRY(launch_build(a, c->precision == DGT_PRECISION_FP64 ? MODE_F64 : MODE_F32, s));
-    DGT_TRY(run_slow(c, a, s));
+    {
+        PhaseTimer t(c, DGT_PHASE_BUILD, s);
+        DGT_TRY(run_build(c, a, s));
+    }
+    {
+        PhaseTimer t(c, DGT_PHASE_SLOW, s);
+        DGT_TRY(run_slow(c, a, s));
+    }
     if (!c->safety) return DGT_OK;
     return conclude(c, s, false);
 }
@@ -400,8 +464,7 @@ int dgt_test_and_repair(dgt_context *c, const double *d_points, int *d_tri, int 
     if (c->n == 0) return DGT_OK;
     if (!d_points || !d_tri || !d_nn || !valid_stride(stride)) return DGT_ERR_INVALID_ARGUMENT;
     cudaStream_t s = (cudaStream_t)stream;
-    c->last_stream = s;
-    c->stats_valid = false;
+    begin_call(c, s);
     DevStatus *dst = c->st.as<DevStatus>();
     DGT_TRY(cudaMemsetAsync(c->st.p, 0, sizeof(DevStatus), s));
     DGT_TRY(run_bin(c, d_points, s));
@@ -420,13 +483,17 @@ int dgt_test_and_repair(dgt_context *c, const double *d_points, int *d_tri, int 
     t.list = lists[0];
     t.list_count = &dst->list_count[0];
     t.st = dst;
-    DGT_TRY(launch_test(t, s));
-    const int mode = c->precision == DGT_PRECISION_FP64 ? MODE_F64 : MODE_F32;
+    {
+        PhaseTimer pt(c, DGT_PHASE_TEST, s);
+        c->launches += 1;
+        DGT_TRY(launch_test(t, s));
+    }
+    phase_begin(c, DGT_PHASE_REPAIR, s);
     int round = 0;
     bool pending = false;
     for (;;) {
         // launch a batch of rounds; each kernel reads its item count on the device
-        int batch = ASYNC_ROUNDS;
+        int batch = round == 0 ? FIRST_ROUNDS : NEXT_ROUNDS;
         for (int b = 0; b < batch; ++b, ++round) {
             int cur = round & 1, nxt = cur ^ 1;
             DGT_TRY(cudaMemsetAsync(&dst->list_count[nxt], 0, sizeof(int), s));
@@ -440,24 +507,25 @@ int dgt_test_and_repair(dgt_context *c, const double *d_points, int *d_tri, int 
             a.epoch = base + round;
             a.next_list = lists[nxt];
             a.next_count = &dst->list_count[nxt];
-            DGT_TRY(launch_build(a, mode, s));
+            DGT_TRY(run_build(c, a, s));
             DGT_TRY(run_slow(c, a, s));
         }
         if (!c->safety) {
             c->epoch = base + round;
-            pending = false;
+            phase_end(c, DGT_PHASE_REPAIR, s);
             return DGT_OK;
         }
         int left = 0;
         DGT_TRY(cudaMemcpyAsync(&left, &dst->list_count[round & 1], sizeof(int), cudaMemcpyDeviceToHost, s));
         DGT_TRY(cudaStreamSynchronize(s));
         if (left == 0) break;
-        if (round > 4 * ASYNC_ROUNDS + 64) {
+        if (round > 256) {
             pending = true;
             break;
         }
     }
     c->epoch = base + round;
+    phase_end(c, DGT_PHASE_REPAIR, s);
     return conclude(c, s, pending);
 }
 
@@ -536,6 +604,33 @@ int dgt_get_stats(dgt_context *c, dgt_stats *out)
         c->stats_valid = true;
     }
     to_stats(*c->h_st, out);
+    out->launches = c->launches;
+    return DGT_OK;
+}
+
+int dgt_set_timing(dgt_context *c, int on)
+{
+    if (!c) return DGT_ERR_INVALID_ARGUMENT;
+    if (on && !c->ev[0][0]) {
+        for (int p = 0; p < DGT_NUM_PHASES; ++p)
+            for (int k = 0; k < 2; ++k) DGT_TRY(cudaEventCreate(&c->ev[p][k]));
+    }
+    c->timing = on != 0;
+    return DGT_OK;
+}
+
+int dgt_get_phase_times(dgt_context *c, double *out_ms)
+{
+    if (!c || !out_ms) return DGT_ERR_INVALID_ARGUMENT;
+    DGT_TRY(cudaStreamSynchronize(c->last_stream));
+    for (int p = 0; p < DGT_NUM_PHASES; ++p) {
+        out_ms[p] = -1.0;
+        if (c->timing && c->ev_used[p]) {
+            float ms = 0.f;
+            DGT_TRY(cudaEventElapsedTime(&ms, c->ev[p][0], c->ev[p][1]));
+            out_ms[p] = ms;
+        }
+    }
     return DGT_OK;
 }
 

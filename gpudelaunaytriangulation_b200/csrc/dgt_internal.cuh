@@ -50,6 +50,7 @@ struct DevStatus {
     unsigned long long insertions;      // ring insertions
     unsigned long long flagged;         // points queued by the test kernel
     unsigned long long repaired;        // points rebuilt by repair rounds
+    unsigned long long cells;           // grid cells scanned
 };
 
 enum : int {
@@ -58,6 +59,9 @@ enum : int {
     EF_SLOW_OVERFLOW = 4,  // a ring outgrew even the large-capacity path
     EF_EXACT_UNRESOLVED = 8,
     EF_BAD_INPUT = 16,     // coordinates not finite
+    // warning, not an error: a certified circle reached past half the box, where minimum-
+    // image offsets stop being unique (the box is too small for that point's Delaunay star)
+    EF_MINIMAGE = 32,
 };
 
 enum : int { MODE_F32 = 0, MODE_F64 = 1 };
@@ -127,7 +131,7 @@ struct TestArgs {
 cudaError_t launch_bin_st(const BinArgs &a, DevStatus *st, cudaStream_t s);
 cudaError_t launch_scan(const int *in, int n, int *bsum, int *out, cudaStream_t s);
 int scan_block_count(int n);
-cudaError_t launch_build(const RingArgs &a, int mode, cudaStream_t s);
+cudaError_t launch_build(const RingArgs &a, int mode, int sms, cudaStream_t s);
 cudaError_t launch_slow(const RingArgs &a, void *scratch, int scratch_items, int capacity, cudaStream_t s);
 cudaError_t launch_test(const TestArgs &a, cudaStream_t s);
 cudaError_t launch_restride(const int *src, int old_stride, int *dst, int new_stride, const int *nn, int n,

@@ -61,7 +61,8 @@ __device__ __forceinline__ double wrap_off(double c, double p, double L, double 
 
 // Circle of a ring edge: {2cx, 2cy, Eb, rc} where c is the centre of the circle through
 // (0, a, b), Eb the per-|d| coefficient of the test bound and rc >= |c| + |c~ - c| a safe
-// radius for scan-region certification.  A degenerate or ill-conditioned edge (gamma <= 0 or
+// radius around c~ for scan-region certification (every point strictly inside the exact
+// circle lies within rc of c~).  A degenerate or ill-conditioned edge (gamma <= 0 or
 // relative error of gamma above 1/8) gets Eb = rc = inf: every test against it is undecided
 // and goes to the float64 recheck.
 //
@@ -93,7 +94,7 @@ __device__ __forceinline__ typename Prec<T>::T4 make_circ(T ax, T ay, T bx, T by
     T E = ((T)3.6 * u * (nxh + nyh) / g + cn * (rho + u)) / ((T)1 - rho);
     E = E * (T)1.1 + P::tiny();
     T eb = (T)2.1 * E + (T)8 * u * cn + P::tiny();
-    T rc = cn * ((T)1 + (T)16 * u) + E;
+    T rc = cn * ((T)1 + (T)16 * u) + (T)2 * E;   // |c| + |c~ - c| <= |c~| + 2E
     if (!(eb < P::inf()) || !(rc < P::inf())) return P::mk4((T)0, (T)0, P::inf(), P::inf());
     return P::mk4(cx2, cy2, eb, rc);
 }

@@ -27,7 +27,7 @@ namespace dgt {
 enum { R_OK = 0, R_CAPACITY = 1, R_EXACT = 2, R_UNBOUNDED = 3, R_NONCONTIG = 4 };
 
 struct Ctr {
-    unsigned cand, tests, u32, u64, ins, mism;
+    unsigned cand, tests, u32, u64, ins, mism, cells;
 };
 
 // ---------------------------------------------------------------- ring storage policies
@@ -87,22 +87,54 @@ __device__ __forceinline__ int wrapi(int i, int n)
     return r < 0 ? r + n : r;
 }
 
-// double offset of ring entry `id` relative to p (virtual corners are exact constants)
-__device__ __forceinline__ double2 entry_off64(const RingArgs &A, const SetDesc &S, double2 p, int id)
-{
-    if (id >= 0) {
-        double2 q = __ldg(&A.pos[id]);
-        return make_double2(wrap_off(q.x, p.x, S.Lx, S.hLx), wrap_off(q.y, p.y, S.Ly, S.hLy));
-    }
-    double V = (double)S.V;
-    int c = -id - 1;   // 0:(V,V) 1:(-V,V) 2:(-V,-V) 3:(V,-V)
-    return make_double2((c == 0 || c == 3) ? V : -V, (c < 2) ? V : -V);
-}
-
 template <typename T>
 __device__ __forceinline__ typename Prec<T>::T2 corner(int c, T V)
 {
     return Prec<T>::mk2((c == 0 || c == 3) ? V : -V, (c < 2) ? V : -V);
+}
+
+// ------------------------------------------------------- out-of-line rare paths (small hot loop)
+// double offset of ring entry `id` relative to p
+__device__ __forceinline__ double2 off64(const double2 *pos, double2 p, double Lx, double hLx, double Ly,
+                                         double hLy, float V, int id)
+{
+    if (id >= 0) {
+        double2 q = __ldg(&pos[id]);
+        return make_double2(wrap_off(q.x, p.x, Lx, hLx), wrap_off(q.y, p.y, Ly, hLy));
+    }
+    int c = -id - 1;   // virtual corners 0:(V,V) 1:(-V,V) 2:(-V,-V) 3:(V,-V)
+    double v = (double)V;
+    return make_double2((c == 0 || c == 3) ? v : -v, (c < 2) ? v : -v);
+}
+
+// float64 in-circle of d against edge (ia, ib); with exact: exact sign when float64 cannot
+// decide.  Returns +1/-1 decided in float64, +2/-2 decided exactly, 0 undecided.
+template <bool EXACT>
+__device__ __noinline__ int recheck64(const double2 *pos, double2 p, double Lx, double hLx, double Ly,
+                                      double hLy, float V, int ia, int ib, double dx, double dy)
+{
+    double2 a = off64(pos, p, Lx, hLx, Ly, hLy, V, ia), b = off64(pos, p, Lx, hLx, Ly, hLy, V, ib);
+    int r = incircle64(a.x, a.y, b.x, b.y, dx, dy);
+    if (r != 0 || !EXACT) return r;
+    r = incircle_exact(a.x, a.y, b.x, b.y, dx, dy);
+    return r > 0 ? 2 : -2;   // on the circle: not strictly inside
+}
+
+// check mode: 1 when float64 certainly contradicts the filter's decision `inside`
+__device__ __noinline__ int check64(const double2 *pos, double2 p, double Lx, double hLx, double Ly, double hLy,
+                                    float V, int ia, int ib, double dx, double dy, int inside)
+{
+    double2 a = off64(pos, p, Lx, hLx, Ly, hLy, V, ia), b = off64(pos, p, Lx, hLx, Ly, hLy, V, ib);
+    int r = incircle64(a.x, a.y, b.x, b.y, dx, dy);
+    return (inside && r < 0) || (!inside && r > 0) ? 1 : 0;
+}
+
+// circle of edge (ia, ib) in double (make_circ layout)
+__device__ __noinline__ double4 circle64(const double2 *pos, double2 p, double Lx, double hLx, double Ly,
+                                         double hLy, float V, int ia, int ib)
+{
+    double2 a = off64(pos, p, Lx, hLx, Ly, hLy, V, ia), b = off64(pos, p, Lx, hLx, Ly, hLy, V, ib);
+    return make_circ<double>(a.x, a.y, b.x, b.y);
 }
 
 // ------------------------------------------------------------------- the construction
@@ -122,6 +154,7 @@ struct Builder {
     int m;
     T r2max;
     int ocx, ocy;
+    bool minimage = false;   // the certified circles reach past half the box
 
     __device__ Builder(const RingArgs &a, const SetDesc &s, Ring &r, Ctr &c, double2 pp, int sl)
         : A(a), S(s), R(r), ctr(c), p(pp), slot(sl), m(0), r2max((T)0), ocx(0), ocy(0) {}
@@ -151,20 +184,14 @@ struct Builder {
         ocy = min(max(cy, 0), S.ysize - 1);
     }
 
-    // float64 (then exact) decision for edge k against candidate d; +1 conflict, -1 none,
-    // 0 undecided (only without EXACT)
-    __device__ int recheck(int k, double2 d64)
+    // float64 (then, on the exact path, exact) decision for edge k against candidate d:
+    // +1 conflict, -1 none, 0 undecided (only without EXACT)
+    __device__ __forceinline__ int recheck(int k, double2 d64)
     {
         int ia = R.idx(k), ib = R.idx(k + 1 == m ? 0 : k + 1);
-        double2 a = entry_off64(A, S, p, ia), b = entry_off64(A, S, p, ib);
-        int r = incircle64(a.x, a.y, b.x, b.y, d64.x, d64.y);
-        if (r != 0) return r;
-        ctr.u64++;
-        if (EXACT) {
-            r = incircle_exact(a.x, a.y, b.x, b.y, d64.x, d64.y);
-            return r > 0 ? 1 : -1;   // on the circle: not strictly inside
-        }
-        return 0;
+        int r = recheck64<EXACT>(A.pos, p, S.Lx, S.hLx, S.Ly, S.hLy, S.V, ia, ib, d64.x, d64.y);
+        if (r == 2 || r == -2 || r == 0) ctr.u64++;
+        return r > 0 ? 1 : (r < 0 ? -1 : 0);
     }
 
     __device__ int insert(V2 d, int id, Mask mask)
@@ -203,147 +230,206 @@ struct Builder {
         return R_OK;
     }
 
-    __device__ int scan_cell(int rx, int ry)
+    // one candidate (cell-order slot sl): filter every ring edge, settle undecided ones,
+    // insert on conflict
+    __device__ __forceinline__ int candidate(int sl)
     {
-        int cx = wrapi(ocx + rx, S.xsize), cy = wrapi(ocy + ry, S.ysize);
-        int c = S.cell_base + cy * S.xsize + cx;
-        int a = __ldg(&A.cstart[c]), b = __ldg(&A.cstart[c + 1]);
-        const T u = PR::u();
-        for (int sl = a; sl < b; ++sl) {
-            if (sl == slot) continue;
-            double2 q = __ldg(&A.spos[sl]);
-            double2 d64 = make_double2(wrap_off(q.x, p.x, S.Lx, S.hLx), wrap_off(q.y, p.y, S.Ly, S.hLy));
-            if (d64.x == 0.0 && d64.y == 0.0) continue;   // coincident point
-            ctr.cand++;
-            V2 d = PR::mk2(PR::from64(d64.x), PR::from64(d64.y));
-            T nd = d.x * d.x + d.y * d.y;
-            if (nd > r2max) continue;
-            T ad = sqrt(nd);
-            T kb = (T)8 * u * nd + PR::tiny();
-            Mask mask = 0;
-            for (int k = 0; k < m; ++k) {
-                E4 e = R.edge(k);
-                T sv = fma(d.x, e.x, fma(d.y, e.y, -nd));
-                T bd = fma(ad, e.z, kb);
-                ctr.tests++;
-                if (sv > bd) {
-                    mask |= (Mask)1 << k;
-                    if (A.check) {
-                        int ia = R.idx(k), ib = R.idx(k + 1 == m ? 0 : k + 1);
-                        double2 aa = entry_off64(A, S, p, ia), bb = entry_off64(A, S, p, ib);
-                        if (incircle64(aa.x, aa.y, bb.x, bb.y, d64.x, d64.y) < 0) ctr.mism++;
-                    }
-                } else if (sv >= -bd) {
-                    ctr.u32++;
-                    int r = recheck(k, d64);
-                    if (r == 0) return R_EXACT;
-                    if (r > 0) mask |= (Mask)1 << k;
-                } else if (A.check) {
-                    int ia = R.idx(k), ib = R.idx(k + 1 == m ? 0 : k + 1);
-                    double2 aa = entry_off64(A, S, p, ia), bb = entry_off64(A, S, p, ib);
-                    if (incircle64(aa.x, aa.y, bb.x, bb.y, d64.x, d64.y) > 0) ctr.mism++;
-                }
-            }
-            if (!mask) continue;
-            int r = insert(d, __ldg(&A.sidx[sl]), mask);
-            if (r != R_OK) return r;
+        if (sl == slot) return R_OK;
+        double2 q = __ldg(&A.spos[sl]);
+        double2 d64 = make_double2(wrap_off(q.x, p.x, S.Lx, S.hLx), wrap_off(q.y, p.y, S.Ly, S.hLy));
+        if (d64.x == 0.0 && d64.y == 0.0) return R_OK;   // coincident point
+        ctr.cand++;
+        V2 d = PR::mk2(PR::from64(d64.x), PR::from64(d64.y));
+        T nd = d.x * d.x + d.y * d.y;
+        if (nd > r2max) return R_OK;
+        T ad = sqrt(nd);
+        T kb = (T)8 * PR::u() * nd + PR::tiny();
+        Mask mask = 0, open = 0;
+        for (int k = 0; k < m; ++k) {
+            E4 e = R.edge(k);
+            T sv = fma(d.x, e.x, fma(d.y, e.y, -nd));
+            T bd = fma(ad, e.z, kb);
+            mask |= (Mask)(sv > bd) << k;
+            open |= (Mask)(sv <= bd && sv >= -bd) << k;
         }
-        return R_OK;
+        ctr.tests += m;
+        if (open) {
+            for (int k = 0; k < m; ++k) {
+                if (!((open >> k) & 1)) continue;
+                ctr.u32++;
+                int r = recheck(k, d64);
+                if (r == 0) return R_EXACT;
+                if (r > 0) mask |= (Mask)1 << k;
+            }
+        }
+        if (A.check) {
+            for (int k = 0; k < m; ++k) {
+                if ((open >> k) & 1) continue;
+                int ia = R.idx(k), ib = R.idx(k + 1 == m ? 0 : k + 1);
+                ctr.mism += check64(A.pos, p, S.Lx, S.hLx, S.Ly, S.hLy, S.V, ia, ib, d64.x, d64.y,
+                                    (int)((mask >> k) & 1));
+            }
+        }
+        if (!mask) return R_OK;
+        return insert(d, __ldg(&A.sidx[sl]), mask);
     }
 
-    // scan the cells of [nx0,nx1]x[ny0,ny1] that are not in [x0,x1]x[y0,y1]
-    __device__ int scan_growth(int x0, int x1, int y0, int y1, int nx0, int nx1, int ny0, int ny1)
+    // Growth of the scanned rectangle from [x0,x1]x[y0,y1] to [nx0,nx1]x[ny0,ny1] by at most
+    // one column / row per side; its new cells are the left column, the right column (over
+    // the old rows), then the bottom and top rows (over the new columns).  own: the single
+    // cell (0,0) of the first phase.
+    struct Growth {
+        int x0, x1, y0, y1, nx0, nx1, ny0, ny1, nl, nr, nb, nt;
+        bool own;
+    };
+    __device__ __forceinline__ static Growth growth(int x0, int x1, int y0, int y1, int nx0, int nx1, int ny0,
+                                                    int ny1, bool own)
     {
-        int r;
-        for (int x = nx0; x < x0; ++x)
-            for (int y = y0; y <= y1; ++y)
-                if ((r = scan_cell(x, y)) != R_OK) return r;
-        for (int x = x1 + 1; x <= nx1; ++x)
-            for (int y = y0; y <= y1; ++y)
-                if ((r = scan_cell(x, y)) != R_OK) return r;
-        for (int y = ny0; y < y0; ++y)
-            for (int x = nx0; x <= nx1; ++x)
-                if ((r = scan_cell(x, y)) != R_OK) return r;
-        for (int y = y1 + 1; y <= ny1; ++y)
-            for (int x = nx0; x <= nx1; ++x)
-                if ((r = scan_cell(x, y)) != R_OK) return r;
-        return R_OK;
+        Growth g{ x0, x1, y0, y1, nx0, nx1, ny0, ny1, 0, 0, 0, 0, own };
+        if (own) return g;
+        g.nl = nx0 < x0 ? (y1 - y0 + 1) : 0;
+        g.nr = nx1 > x1 ? (y1 - y0 + 1) : 0;
+        g.nb = ny0 < y0 ? (nx1 - nx0 + 1) : 0;
+        g.nt = ny1 > y1 ? (nx1 - nx0 + 1) : 0;
+        return g;
+    }
+    __device__ __forceinline__ static void growth_cell(const Growth &g, int ci, int &rx, int &ry)
+    {
+        if (g.own) { rx = 0; ry = 0; return; }
+        if (ci < g.nl) { rx = g.x0 - 1; ry = g.y0 + ci; return; }
+        ci -= g.nl;
+        if (ci < g.nr) { rx = g.x1 + 1; ry = g.y0 + ci; return; }
+        ci -= g.nr;
+        if (ci < g.nb) { rx = g.nx0 + ci; ry = g.y0 - 1; return; }
+        ci -= g.nb;
+        rx = g.nx0 + ci;
+        ry = g.y1 + 1;
     }
 
-    // circle of edge k in double: centre (relative) and safe radius; false if degenerate
-    __device__ bool circle64(int k, double &cx, double &cy, double &rc)
+    // every candidate of the growth's cells.  The lanes of a warp advance in lockstep, one
+    // candidate each per step (a warp vote closes every step), so the candidate code runs
+    // with all lanes that still have candidates.  Every lane of the warp must call this;
+    // `live` is false for lanes with nothing to scan.
+    __device__ __forceinline__ int scan(const Growth &g, bool live)
     {
-        int ia = R.idx(k), ib = R.idx(k + 1 == m ? 0 : k + 1);
-        double2 a = entry_off64(A, S, p, ia), b = entry_off64(A, S, p, ib);
-        double4 c = make_circ<double>(a.x, a.y, b.x, b.y);
-        if (!(c.w < Prec<double>::inf())) return false;
-        cx = 0.5 * c.x;
-        cy = 0.5 * c.y;
-        rc = c.w;
+        const int ncell = !live ? 0 : (g.own ? 1 : g.nl + g.nr + g.nb + g.nt);
+        int ci = 0, sl = 0, se = 0, status = R_OK;
+        for (;;) {
+            bool have = false;
+            if (status == R_OK) {
+                while (sl >= se && ci < ncell) {
+                    int rx, ry;
+                    growth_cell(g, ci++, rx, ry);
+                    int cx = wrapi(ocx + rx, S.xsize), cy = wrapi(ocy + ry, S.ysize);
+                    int c = S.cell_base + cy * S.xsize + cx;
+                    ctr.cells++;
+                    sl = __ldg(&A.cstart[c]);
+                    se = __ldg(&A.cstart[c + 1]);
+                }
+                have = sl < se;
+            }
+            if (!__any_sync(0xffffffffu, have)) break;
+            if (have) {
+                int r = candidate(sl++);
+                if (r != R_OK) status = r;
+            }
+        }
+        return status;
+    }
+
+    // Certification: cells (relative to the own cell) covering the union of the edge circles'
+    // bounding boxes.  Returns false when some circle cannot be bounded (whole box needed).
+    __device__ bool need_rect(double fx, double fy, int &lx, int &hx, int &ly, int &hy)
+    {
+        double xmin = 1e300, xmax = -1e300, ymin = 1e300, ymax = -1e300;
+        for (int k = 0; k < m; ++k) {
+            E4 e = R.edge(k);
+            double cx, cy, rc;
+            if (e.w < PR::inf()) {
+                cx = 0.5 * (double)e.x;
+                cy = 0.5 * (double)e.y;
+                rc = (double)e.w;
+            } else {
+                int ia = R.idx(k), ib = R.idx(k + 1 == m ? 0 : k + 1);
+                double4 c = circle64(A.pos, p, S.Lx, S.hLx, S.Ly, S.hLy, S.V, ia, ib);
+                if (!(c.w < Prec<double>::inf())) {
+                    minimage = true;
+                    return false;
+                }
+                cx = 0.5 * c.x;
+                cy = 0.5 * c.y;
+                rc = c.w;
+            }
+            xmin = fmin(xmin, cx - rc);
+            xmax = fmax(xmax, cx + rc);
+            ymin = fmin(ymin, cy - rc);
+            ymax = fmax(ymax, cy + rc);
+        }
+        // judged on the circles of the latest ring only (the final one when the scan ends)
+        minimage = xmin < -S.hLx || xmax > S.hLx || ymin < -S.hLy || ymax > S.hLy;
+        double a0 = fx + xmin * S.icw, a1 = fx + xmax * S.icw;
+        double b0 = fy + ymin * S.ich, b1 = fy + ymax * S.ich;
+        a0 -= 1e-9 * (1.0 + fabs(a0));
+        a1 += 1e-9 * (1.0 + fabs(a1));
+        b0 -= 1e-9 * (1.0 + fabs(b0));
+        b1 += 1e-9 * (1.0 + fabs(b1));
+        lx = (int)fmax(floor(a0), -1e8);
+        hx = (int)fmin(floor(a1), 1e8);
+        ly = (int)fmax(floor(b0), -1e8);
+        hy = (int)fmin(floor(b1), 1e8);
         return true;
     }
 
-    __device__ int run()
+    // Called by every lane of the warp (warp votes inside); `active` false for lanes
+    // without a point.  Returns R_OK / error for active lanes.
+    __device__ int run(bool active)
     {
         init();
-        int r = scan_cell(0, 0);
-        if (r != R_OK) return r;
-        int x0 = 0, x1 = 0, y0 = 0, y1 = 0;
-        // the 3x3 block (fewer columns/rows on grids narrower than 3 cells)
-        int nx0 = S.xsize >= 3 ? -1 : 0, nx1 = S.xsize >= 2 ? 1 : 0;
-        int ny0 = S.ysize >= 3 ? -1 : 0, ny1 = S.ysize >= 2 ? 1 : 0;
-        r = scan_growth(x0, x1, y0, y1, nx0, nx1, ny0, ny1);
-        if (r != R_OK) return r;
-        x0 = nx0; x1 = nx1; y0 = ny0; y1 = ny1;
         const double fx = p.x * S.icw - (double)ocx, fy = p.y * S.ich - (double)ocy;
-        for (int it = 0; it < S.xsize + S.ysize + 8; ++it) {
-            // union of the edge circles' bounding boxes, in cells relative to the own cell
-            double xmin = 1e300, xmax = -1e300, ymin = 1e300, ymax = -1e300;
-            bool full = false;
-            for (int k = 0; k < m && !full; ++k) {
-                E4 e = R.edge(k);
-                double cx, cy, rc;
-                if (e.w < PR::inf()) {
-                    cx = 0.5 * (double)e.x;
-                    cy = 0.5 * (double)e.y;
-                    rc = (double)e.w;
-                } else if (!circle64(k, cx, cy, rc)) {
-                    full = true;
-                    break;
-                }
-                xmin = fmin(xmin, cx - rc);
-                xmax = fmax(xmax, cx + rc);
-                ymin = fmin(ymin, cy - rc);
-                ymax = fmax(ymax, cy + rc);
-            }
-            int lx, hx, ly, hy;
-            if (full) {
-                lx = ly = -(1 << 28);
-                hx = hy = (1 << 28);
-            } else {
-                double a0 = fx + xmin * S.icw, a1 = fx + xmax * S.icw;
-                double b0 = fy + ymin * S.ich, b1 = fy + ymax * S.ich;
-                a0 -= 1e-9 * (1.0 + fabs(a0));
-                a1 += 1e-9 * (1.0 + fabs(a1));
-                b0 -= 1e-9 * (1.0 + fabs(b0));
-                b1 += 1e-9 * (1.0 + fabs(b1));
-                lx = (int)fmax(floor(a0), -1e8);
-                hx = (int)fmin(floor(a1), 1e8);
-                ly = (int)fmax(floor(b0), -1e8);
-                hy = (int)fmin(floor(b1), 1e8);
-            }
+        int x0 = 0, x1 = 0, y0 = 0, y1 = 0;
+        const int max_phase = S.xsize + S.ysize + 8;
+        bool done = !active;
+        int status = R_OK;
+        for (int phase = 0;; ++phase) {
+            bool live = !done && status == R_OK;
             int gx0 = x0, gx1 = x1, gy0 = y0, gy1 = y1;
-            if (lx < x0 && gx1 - gx0 + 1 < S.xsize) gx0--;
-            if (hx > x1 && gx1 - gx0 + 1 < S.xsize) gx1++;
-            if (ly < y0 && gy1 - gy0 + 1 < S.ysize) gy0--;
-            if (hy > y1 && gy1 - gy0 + 1 < S.ysize) gy1++;
-            if (gx0 == x0 && gx1 == x1 && gy0 == y0 && gy1 == y1) break;
-            r = scan_growth(x0, x1, y0, y1, gx0, gx1, gy0, gy1);
-            if (r != R_OK) return r;
-            x0 = gx0; x1 = gx1; y0 = gy0; y1 = gy1;
+            if (live && phase >= max_phase) {
+                done = true;
+                live = false;
+            }
+            if (live && phase == 1) {
+                // the 3x3 block (fewer columns / rows on grids narrower than 3 cells)
+                gx0 = S.xsize >= 3 ? -1 : 0;
+                gx1 = S.xsize >= 2 ? 1 : 0;
+                gy0 = S.ysize >= 3 ? -1 : 0;
+                gy1 = S.ysize >= 2 ? 1 : 0;
+            } else if (live && phase > 1) {
+                int lx, hx, ly, hy;
+                if (!need_rect(fx, fy, lx, hx, ly, hy)) {
+                    lx = ly = -(1 << 28);
+                    hx = hy = (1 << 28);
+                }
+                if (lx < x0 && gx1 - gx0 + 1 < S.xsize) gx0--;
+                if (hx > x1 && gx1 - gx0 + 1 < S.xsize) gx1++;
+                if (ly < y0 && gy1 - gy0 + 1 < S.ysize) gy0--;
+                if (hy > y1 && gy1 - gy0 + 1 < S.ysize) gy1++;
+                if (gx0 == x0 && gx1 == x1 && gy0 == y0 && gy1 == y1) {
+                    done = true;
+                    live = false;
+                }
+            }
+            int r = scan(growth(x0, x1, y0, y1, gx0, gx1, gy0, gy1, phase == 0), live);
+            if (live) {
+                if (r != R_OK) status = r;
+                x0 = gx0; x1 = gx1; y0 = gy0; y1 = gy1;
+            }
+            if (__all_sync(0xffffffffu, done || status != R_OK)) break;
         }
+        if (!active) return R_OK;
+        if (status != R_OK) return status;
         for (int k = 0; k < m; ++k)
             if (R.idx(k) < 0) return R_UNBOUNDED;
+        if (minimage) atomicOr(&A.st->err_flags, EF_MINIMAGE);
         return R_OK;
     }
 };
@@ -408,8 +494,8 @@ __device__ void finish(const RingArgs &A, int pid, Ring &R, int m, int &maxr)
 
 __device__ __forceinline__ void flush_counters(const RingArgs &A, const Ctr &c, unsigned pts, int maxr)
 {
-    unsigned long long v[7] = { pts, c.cand, c.tests, c.u32, c.u64, c.ins, c.mism };
-    for (int i = 0; i < 7; ++i)
+    unsigned long long v[8] = { pts, c.cand, c.tests, c.u32, c.u64, c.ins, c.mism, c.cells };
+    for (int i = 0; i < 8; ++i)
         for (int o = 16; o > 0; o >>= 1) v[i] += __shfl_down_sync(0xffffffffu, v[i], o);
     for (int o = 16; o > 0; o >>= 1) maxr = max(maxr, __shfl_down_sync(0xffffffffu, maxr, o));
     if ((threadIdx.x & 31) == 0) {
@@ -420,6 +506,7 @@ __device__ __forceinline__ void flush_counters(const RingArgs &A, const Ctr &c, 
         if (v[4]) atomicAdd(&A.st->f64_undecided, v[4]);
         if (v[5]) atomicAdd(&A.st->insertions, v[5]);
         if (v[6]) atomicAdd(&A.st->mismatches, v[6]);
+        if (v[7]) atomicAdd(&A.st->cells, v[7]);
         if (maxr > 0) atomicMax(&A.st->max_ring, maxr);
     }
 }
@@ -441,7 +528,7 @@ __global__ void __launch_bounds__(BLOCK) k_build(RingArgs A)
     __shared__ V2 sv[CAP][BLOCK];
     __shared__ int si[CAP][BLOCK];
     SmemRing<T, CAP, BLOCK> ring{ se, sv, si, (int)threadIdx.x };
-    Ctr ctr = { 0, 0, 0, 0, 0, 0 };
+    Ctr ctr = { 0, 0, 0, 0, 0, 0, 0 };
     unsigned pts = 0;
     int maxr = 0;
     const int n = item_count(A);
@@ -450,9 +537,11 @@ __global__ void __launch_bounds__(BLOCK) k_build(RingArgs A)
         atomicMax(&A.st->rounds, A.epoch - A.epoch_base + 1);
     }
     for (int base = blockIdx.x * BLOCK; base < n; base += gridDim.x * BLOCK) {
+        // every lane runs the builder (it votes across the warp); lanes past the end idle
         int t = base + threadIdx.x;
-        if (t < n) {
-            int pid, slot;
+        const bool act = t < n;
+        int pid = -1, slot = -1;
+        if (act) {
             if (A.worklist) {
                 pid = A.worklist[t];
                 slot = A.slot_of[pid];
@@ -460,10 +549,12 @@ __global__ void __launch_bounds__(BLOCK) k_build(RingArgs A)
                 slot = t;
                 pid = __ldg(&A.sidx[t]);
             }
-            const SetDesc S = A.sets[A.set_of ? __ldg(&A.set_of[slot]) : 0];
-            double2 p = __ldg(&A.spos[slot]);
-            Builder<T, false, SmemRing<T, CAP, BLOCK>> b(A, S, ring, ctr, p, slot);
-            int r = b.run();
+        }
+        const SetDesc S = A.sets[(act && A.set_of) ? __ldg(&A.set_of[slot]) : 0];
+        double2 p = act ? __ldg(&A.spos[slot]) : make_double2(0.0, 0.0);
+        Builder<T, false, SmemRing<T, CAP, BLOCK>> b(A, S, ring, ctr, p, slot);
+        int r = b.run(act);
+        if (act) {
             pts++;
             if (r == R_OK) {
                 finish(A, pid, ring, b.m, maxr);
@@ -492,7 +583,7 @@ struct SlowRow {
 __global__ void __launch_bounds__(64) k_build_slow(RingArgs A, SlowRow<double> *scratch, int scratch_items)
 {
     int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    Ctr ctr = { 0, 0, 0, 0, 0, 0 };
+    Ctr ctr = { 0, 0, 0, 0, 0, 0, 0 };
     unsigned pts = 0;
     int maxr = 0;
     const int n = *A.slow_count;
@@ -500,15 +591,16 @@ __global__ void __launch_bounds__(64) k_build_slow(RingArgs A, SlowRow<double> *
     const int rounds = (n + nthreads - 1) / nthreads;
     for (int rd = 0; rd < rounds; ++rd) {
         int t = rd * nthreads + tid;
-        if (t < n && tid < scratch_items) {
-            int pid = A.slow_list[t];
-            int slot = A.slot_of[pid];
-            const SetDesc S = A.sets[A.set_of ? A.set_of[slot] : 0];
-            double2 p = A.spos[slot];
-            SlowRow<double> &row = scratch[tid];
-            GlobalRing<double, SLOW_CAP> ring{ row.e, row.v, row.id };
-            Builder<double, true, GlobalRing<double, SLOW_CAP>> b(A, S, ring, ctr, p, slot);
-            int r = b.run();
+        const bool act = t < n && tid < scratch_items;
+        int pid = act ? A.slow_list[t] : -1;
+        int slot = act ? A.slot_of[pid] : -1;
+        const SetDesc S = A.sets[(act && A.set_of) ? A.set_of[slot] : 0];
+        double2 p = act ? A.spos[slot] : make_double2(0.0, 0.0);
+        SlowRow<double> &row = scratch[tid < scratch_items ? tid : 0];
+        GlobalRing<double, SLOW_CAP> ring{ row.e, row.v, row.id };
+        Builder<double, true, GlobalRing<double, SLOW_CAP>> b(A, S, ring, ctr, p, slot);
+        int r = b.run(act);
+        if (act) {
             pts++;
             if (r == R_OK) {
                 finish(A, pid, ring, b.m, maxr);
@@ -632,13 +724,10 @@ __global__ void __launch_bounds__(256) k_test(TestArgs A)
 
 // ------------------------------------------------------------------------- launchers
 template <typename T, int CAP, int BLOCK>
-static cudaError_t launch_build_t(const RingArgs &a, cudaStream_t s)
+static cudaError_t launch_build_t(const RingArgs &a, int sms, cudaStream_t s)
 {
     int blocks;
     if (a.worklist) {
-        int dev = 0, sms = 148;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         int want = (a.n_items + BLOCK - 1) / BLOCK;
         blocks = want < sms * 32 ? want : sms * 32;
     } else {
@@ -649,11 +738,11 @@ static cudaError_t launch_build_t(const RingArgs &a, cudaStream_t s)
     return cudaGetLastError();
 }
 
-cudaError_t launch_build(const RingArgs &a, int mode, cudaStream_t s)
+cudaError_t launch_build(const RingArgs &a, int mode, int sms, cudaStream_t s)
 {
     if (a.n_items <= 0) return cudaSuccess;
-    if (mode == MODE_F64) return launch_build_t<double, 14, 64>(a, s);
-    return launch_build_t<float, 14, 64>(a, s);
+    if (mode == MODE_F64) return launch_build_t<double, 14, 64>(a, sms, s);
+    return launch_build_t<float, 14, 64>(a, sms, s);
 }
 
 cudaError_t launch_slow(const RingArgs &a, void *scratch, int scratch_items, int, cudaStream_t s)

@@ -21,7 +21,7 @@ from dataclasses import dataclass
 
 import torch
 
-from . import _native as N
+from . import _native as _nat
 
 
 @dataclass
@@ -69,13 +69,13 @@ class DelaunayGPU:
 
     def __init__(self, N: int, maximumNeighborsGuess: int = 16, cellSize: float = 1.0,
                  box: PeriodicBox | tuple | None = None, *, _batch=None):
-        self._L = N_lib = N.lib()
+        self._L = lib = _nat.lib()
         self._h = ctypes.c_void_p()
         if _batch is not None:
             sizes, boxes, rel_cell = _batch
             sz = (ctypes.c_int * len(sizes))(*[int(s) for s in sizes])
             bx = (ctypes.c_double * (2 * len(sizes)))(*[float(v) for b in boxes for v in b])
-            N.check(N_lib.dgt_create_batch(len(sizes), sz, bx, float(rel_cell), int(maximumNeighborsGuess),
+            _nat.check(lib.dgt_create_batch(len(sizes), sz, bx, float(rel_cell), int(maximumNeighborsGuess),
                                            ctypes.byref(self._h)), "dgt_create_batch")
             self.Ncells = int(sum(int(s) for s in sizes))
             self.Box = None
@@ -86,7 +86,7 @@ class DelaunayGPU:
                 box = PeriodicBox(float(box[0]), float(box[1]))
             self.Box = box
             self.Ncells = int(N)
-            N.check(N_lib.dgt_create(self.Ncells, int(maximumNeighborsGuess), float(cellSize), box.Lx, box.Ly,
+            _nat.check(lib.dgt_create(self.Ncells, int(maximumNeighborsGuess), float(cellSize), box.Lx, box.Ly,
                                      ctypes.byref(self._h)), "dgt_create")
         self.safetyMode = True
         self.GPUcompute = True
@@ -96,25 +96,25 @@ class DelaunayGPU:
     @property
     def MaxSize(self) -> int:
         v = ctypes.c_int()
-        N.check(self._L.dgt_get_max_size(self._h, ctypes.byref(v)), "dgt_get_max_size")
+        _nat.check(self._L.dgt_get_max_size(self._h, ctypes.byref(v)), "dgt_get_max_size")
         return v.value
 
     def resize(self, nmax: int):
         """resize(nmax) (DelaunayGPU.h:38): the ring capacity MaxSize."""
-        N.check(self._L.dgt_resize(self._h, int(nmax)), "dgt_resize")
+        _nat.check(self._L.dgt_resize(self._h, int(nmax)), "dgt_resize")
 
     def setCellListSize(self, csize: float):
-        N.check(self._L.dgt_set_cell_size(self._h, float(csize)), "dgt_set_cell_size")
+        _nat.check(self._L.dgt_set_cell_size(self._h, float(csize)), "dgt_set_cell_size")
 
     def setBox(self, box: PeriodicBox | tuple):
         if not isinstance(box, PeriodicBox):
             box = PeriodicBox(float(box[0]), float(box[1]))
-        N.check(self._L.dgt_set_box(self._h, box.Lx, box.Ly), "dgt_set_box")
+        _nat.check(self._L.dgt_set_box(self._h, box.Lx, box.Ly), "dgt_set_box")
         self.Box = box
 
     def setSafetyMode(self, flag: bool):
         self.safetyMode = bool(flag)
-        N.check(self._L.dgt_set_safety_mode(self._h, 1 if flag else 0), "dgt_set_safety_mode")
+        _nat.check(self._L.dgt_set_safety_mode(self._h, 1 if flag else 0), "dgt_set_safety_mode")
 
     def setGPUcompute(self, flag: bool):
         """The reference can run its OpenMP host path instead; this library has no CPU path."""
@@ -127,16 +127,16 @@ class DelaunayGPU:
         return None
 
     def setPrecision(self, fp32_filter: bool = True):
-        N.check(self._L.dgt_set_precision(self._h, N.PRECISION_FP32_FILTER if fp32_filter else N.PRECISION_FP64),
+        _nat.check(self._L.dgt_set_precision(self._h, _nat.PRECISION_FP32_FILTER if fp32_filter else _nat.PRECISION_FP64),
                 "dgt_set_precision")
 
     def setCheckMode(self, on: bool):
-        N.check(self._L.dgt_set_check_mode(self._h, 1 if on else 0), "dgt_set_check_mode")
+        _nat.check(self._L.dgt_set_check_mode(self._h, 1 if on else 0), "dgt_set_check_mode")
 
     # ------------------------------------------------------------------------- the path
     def updateList(self, points: torch.Tensor, stream=None):
         _check_points(points, self.Ncells)
-        N.check(self._L.dgt_update_list(self._h, _ptr(points), _stream_ptr(stream)), "dgt_update_list")
+        _nat.check(self._L.dgt_update_list(self._h, _ptr(points), _stream_ptr(stream)), "dgt_update_list")
 
     def _fit(self, tri: torch.Tensor | None, nn: torch.Tensor | None, device):
         n = self.Ncells
@@ -163,10 +163,10 @@ class DelaunayGPU:
             stride = tri.numel() // n
             code = self._L.dgt_global_triangulation(self._h, _ptr(points), _ptr(tri), _ptr(nn), stride,
                                                     _stream_ptr(stream))
-            if code == N.DGT_ERR_NEED_RESIZE and self.safetyMode:
+            if code == _nat.DGT_ERR_NEED_RESIZE and self.safetyMode:
                 tri.resize_(self.MaxSize * n)   # DelaunayGPU.cpp:152-155 grows and recomputes
                 continue
-            N.check(code, "globalDelaunayTriangulation")
+            _nat.check(code, "globalDelaunayTriangulation")
             break
         return tri, nn
 
@@ -183,28 +183,38 @@ class DelaunayGPU:
             stride = tri.numel() // n
             code = self._L.dgt_test_and_repair(self._h, _ptr(points), _ptr(tri), _ptr(nn), stride,
                                                _stream_ptr(stream))
-            if code == N.DGT_ERR_NEED_RESIZE and self.safetyMode:
+            if code == _nat.DGT_ERR_NEED_RESIZE and self.safetyMode:
                 # re-stride every row into the larger array (rows keep their contents;
                 # the reference copies linearly here, DelaunayGPU.cpp:109-112), then go on
                 new = torch.zeros(self.MaxSize * n, dtype=torch.int32, device=tri.device)
-                N.check(self._L.dgt_restride(_ptr(tri), stride, _ptr(new), self.MaxSize, _ptr(nn), n,
+                _nat.check(self._L.dgt_restride(_ptr(tri), stride, _ptr(new), self.MaxSize, _ptr(nn), n,
                                              _stream_ptr(stream)), "dgt_restride")
                 tri.resize_(new.numel())
                 tri.copy_(new)
                 continue
-            N.check(code, "testAndRepairDelaunayTriangulation")
+            _nat.check(code, "testAndRepairDelaunayTriangulation")
             break
         return tri, nn
 
     def displace(self, points: torch.Tensor, sigma: float, seed: int, step: int, stream=None):
         """MD-like step helper: Gaussian displacement + periodic wrap on the device."""
         _check_points(points, self.Ncells)
-        N.check(self._L.dgt_displace(self._h, _ptr(points), float(sigma), int(seed) & (2**64 - 1),
+        _nat.check(self._L.dgt_displace(self._h, _ptr(points), float(sigma), int(seed) & (2**64 - 1),
                                      int(step) & (2**64 - 1), _stream_ptr(stream)), "dgt_displace")
 
+    def setTiming(self, on: bool):
+        """Record CUDA events around each phase of every call (see phaseTimes)."""
+        _nat.check(self._L.dgt_set_timing(self._h, 1 if on else 0), "dgt_set_timing")
+
+    def phaseTimes(self) -> dict:
+        """Milliseconds per phase of the last call (None for phases it did not run)."""
+        out = (ctypes.c_double * len(_nat.PHASES))()
+        _nat.check(self._L.dgt_get_phase_times(self._h, out), "dgt_get_phase_times")
+        return {name: (v if v >= 0 else None) for name, v in zip(_nat.PHASES, out)}
+
     def stats(self) -> dict:
-        s = N.Stats()
-        N.check(self._L.dgt_get_stats(self._h, ctypes.byref(s)), "dgt_get_stats")
+        s = _nat.Stats()
+        _nat.check(self._L.dgt_get_stats(self._h, ctypes.byref(s)), "dgt_get_stats")
         self.last_stats = s.as_dict()
         return self.last_stats
 

@@ -47,11 +47,31 @@ typedef struct dgt_stats {
     long long insertions;      /* ring insertions */
     long long flagged;         /* test-and-repair: points flagged by the local test */
     long long repaired;        /* test-and-repair: points rebuilt (all rounds) */
+    long long cells;           /* grid cells scanned */
     int repair_rounds;         /* test-and-repair: rounds until no ring changed */
     int max_ring;              /* largest ring of the call */
-    int error_flags;
-    int reserved;
+    int error_flags;           /* DGT_FLAG_* bits */
+    int launches;              /* kernels this library launched in the call */
 } dgt_stats;
+
+/* phases timed with CUDA events when timing is on (dgt_set_timing) */
+#define DGT_PHASE_BIN 0        /* cell grid: count, scan, scatter, in-cell order */
+#define DGT_PHASE_BUILD 1      /* one-ring kernel over all points (global triangulation) */
+#define DGT_PHASE_SLOW 2       /* exact / large-ring path */
+#define DGT_PHASE_TEST 3       /* local Delaunay test (test-and-repair) */
+#define DGT_PHASE_REPAIR 4     /* all repair rounds (test-and-repair) */
+#define DGT_NUM_PHASES 5
+
+/* dgt_stats.error_flags */
+#define DGT_FLAG_UNBOUNDED 1    /* a ring kept a virtual corner after scanning the whole box */
+#define DGT_FLAG_NONCONTIG 2    /* degenerate conflict set (duplicate / cocircular input) */
+#define DGT_FLAG_RING_OVERFLOW 4 /* a ring outgrew the large-ring path (64) */
+#define DGT_FLAG_UNRESOLVED 8
+#define DGT_FLAG_BAD_POINTS 16
+/* warning only: some Delaunay circle reached past half the box, where minimum-image
+   offsets are no longer unique (the reference has the same limit); results for such
+   points follow the minimum-image convention */
+#define DGT_FLAG_MINIMUM_IMAGE 32
 
 /* DelaunayGPU(int N, int maximumNeighborsGuess, double cellSize, PeriodicBoxPtr bx)
  * (src/model/DelaunayGPU.h:25, DelaunayGPU.cpp:11-37).  Rectangular periodic box Lx x Ly.
@@ -109,6 +129,12 @@ int dgt_restride(const int *d_src, int src_stride, int *d_dst, int dst_stride, c
 
 /* Counters of the last call (synchronises the context's last stream). */
 int dgt_get_stats(dgt_context *ctx, dgt_stats *out);
+
+/* 1: record CUDA events around each phase of every call (on the call's stream). */
+int dgt_set_timing(dgt_context *ctx, int on);
+/* Milliseconds per phase of the last call (DGT_NUM_PHASES values, -1 for phases the call did
+ * not run); synchronises the last stream. */
+int dgt_get_phase_times(dgt_context *ctx, double *out_ms);
 
 /* MD-like helper: every point += sigma * N(0,1) per axis (counter-based normals of
  * (seed, step, index)), wrapped into its box (periodicBoundaries::move,

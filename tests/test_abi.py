@@ -66,3 +66,14 @@ def test_cpp_adapter_header_compiles(tmp_path):
     r = subprocess.run(["g++", "-std=c++14", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), "-I", cuda_inc,
                         str(src)], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_python_mirror_fails_loudly_without_device():
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    from gpudelaunaytriangulation_b200.delaunay import DelaunayGPU
+
+    with pytest.raises(N.DgtError) as e:
+        DelaunayGPU(10, 16, 1.0, (3.0, 3.0))
+    assert e.value.code == N.DGT_ERR_CUDA
