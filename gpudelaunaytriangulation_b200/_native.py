@@ -30,8 +30,9 @@ EXPORTED = [
     "dgt_update_list", "dgt_set_cell_size", "dgt_set_box", "dgt_set_safety_mode", "dgt_set_precision",
     "dgt_set_check_mode", "dgt_resize", "dgt_get_max_size", "dgt_get_num_points", "dgt_restride",
     "dgt_get_stats", "dgt_displace", "dgt_error_string", "dgt_version", "dgt_set_timing",
-    "dgt_get_phase_times",
+    "dgt_get_phase_times", "dgt_global_triangulation_noalloc",
 ]
+NOALLOC_MAX_POINTS = 65536
 PHASES = ["bin", "build", "slow", "test", "repair"]
 
 
@@ -111,6 +112,8 @@ def lib() -> ctypes.CDLL:
     L.dgt_version.restype = ctypes.c_int
     L.dgt_set_timing.argtypes = [vp, ctypes.c_int]
     L.dgt_get_phase_times.argtypes = [vp, P_D]
+    L.dgt_global_triangulation_noalloc.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                                   ctypes.c_double, vp, vp, ctypes.c_int, P_I, vp]
     _lib = L
     return L
 

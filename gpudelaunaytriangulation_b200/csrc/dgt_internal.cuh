@@ -139,5 +139,7 @@ cudaError_t launch_restride(const int *src, int old_stride, int *dst, int new_st
 cudaError_t launch_displace(double2 *pos, int n, const SetDesc *sets, const int *set_of, double sigma,
                             unsigned long long seed, unsigned long long step, cudaStream_t s);
 size_t slow_scratch_bytes_per_item(int capacity);
+// bytes of one row of the exact / large-ring path (64 entries of double4 + double2 + int)
+constexpr size_t SLOW_ROW_BYTES = 64 * (sizeof(double4) + sizeof(double2) + sizeof(int));
 
 }  // namespace dgt

@@ -1,0 +1,202 @@
+// Global triangulation without any device allocation (dgt_global_triangulation_noalloc).
+//
+// Some callers cannot call cudaMalloc: code running where the allocator is owned by
+// someone else (a host application with its own pool that forbids side allocations,
+// plugins loaded into a process whose memory budget is fixed up front, or paths that must
+// not touch the allocator at all).  This entry point keeps every piece of scratch it needs
+// (cell grid, cell-order copies, status block, rows of the exact / large-ring path) in one
+// file-scope device array of fixed size, so a call allocates nothing: the caller passes the
+// points, the output rows and the output lengths, nothing else is needed.
+//
+// Limits: at most DGT_NOALLOC_MAX_POINTS points and DGT_NOALLOC_MAX_CELLS grid cells; larger
+// inputs are rejected with DGT_ERR_INVALID_ARGUMENT before any work is queued.  The array
+// (about 4.8 MB) exists on every GPU that loads this library, until the process exits.
+//
+// Sharing: all calls use the same array and it keeps the last call's contents; the parts
+// that must start at zero (cell counts, status block) are cleared by every call.  Calls
+// whose kernels overlap on a GPU (different streams or host threads without ordering)
+// race on the array; callers must order them.
+//
+// Set-up: the first call on a device, with that device current, looks the array's
+// device address up once (cudaGetSymbolAddress; host code cannot use the array's name as a
+// device pointer) and caches it per device.  Make that first call before any stream capture.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+
+#include "dgt.h"
+#include "dgt_internal.cuh"
+
+using namespace dgt;
+
+namespace {
+
+constexpr int NA_MAX_POINTS = DGT_NOALLOC_MAX_POINTS;
+constexpr int NA_MAX_CELLS = DGT_NOALLOC_MAX_CELLS;
+constexpr int NA_SLOW_ITEMS = 64;
+constexpr size_t NA_ALIGN = 256;
+
+constexpr size_t up(size_t x) { return (x + NA_ALIGN - 1) / NA_ALIGN * NA_ALIGN; }
+
+// byte offsets of each region inside the array
+constexpr size_t OFF_SETS = 0;
+constexpr size_t OFF_STATUS = OFF_SETS + up(sizeof(SetDesc));
+constexpr size_t OFF_CCOUNT = OFF_STATUS + up(sizeof(DevStatus));
+constexpr size_t OFF_CSTART = OFF_CCOUNT + up(sizeof(int) * (NA_MAX_CELLS + 1));
+constexpr size_t OFF_BSUM = OFF_CSTART + up(sizeof(int) * (NA_MAX_CELLS + 1));
+constexpr size_t OFF_CELLOF = OFF_BSUM + up(sizeof(int) * ((NA_MAX_CELLS + 1) / 4096 + 2));
+constexpr size_t OFF_RANK = OFF_CELLOF + up(sizeof(int) * NA_MAX_POINTS);
+constexpr size_t OFF_SIDX = OFF_RANK + up(sizeof(int) * NA_MAX_POINTS);
+constexpr size_t OFF_SLOTOF = OFF_SIDX + up(sizeof(int) * NA_MAX_POINTS);
+constexpr size_t OFF_SLOWLIST = OFF_SLOTOF + up(sizeof(int) * NA_MAX_POINTS);
+constexpr size_t OFF_SPOS = OFF_SLOWLIST + up(sizeof(int) * NA_MAX_POINTS);
+constexpr size_t OFF_SLOWROWS = OFF_SPOS + up(sizeof(double2) * NA_MAX_POINTS);
+constexpr size_t NA_BYTES = OFF_SLOWROWS + up(SLOW_ROW_BYTES * NA_SLOW_ITEMS);
+
+}  // namespace
+
+// the scratch array itself (device code could name it directly; host code needs its address)
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
+
+namespace {
+
+constexpr int NA_MAX_DEVICES = 64;
+unsigned char *g_base[NA_MAX_DEVICES] = {};
+std::mutex g_setup_mutex;
+
+// once per device, with that device current: the array's device address
+int scratch_base(int dev, unsigned char **out)
+{
+    if (dev < 0 || dev >= NA_MAX_DEVICES) return DGT_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    if (!g_base[dev]) {
+        void *ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || !ptr) return DGT_ERR_CUDA;
+        g_base[dev] = static_cast<unsigned char *>(ptr);
+    }
+    *out = g_base[dev];
+    return DGT_OK;
+}
+
+double pow2_at_least(double x)
+{
+    double v = 1.0;
+    while (v < x) v *= 2.0;
+    return v;
+}
+
+}  // namespace
+
+// writes the set descriptor and clears what must start at zero (cell counts, status)
+__global__ void k_noalloc_setup(SetDesc S, SetDesc *sets, DevStatus *st, int *ccount, int ncount)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        *sets = S;
+        *st = DevStatus();
+    }
+    for (; i < ncount; i += gridDim.x * blockDim.x) ccount[i] = 0;
+}
+
+extern "C" int dgt_global_triangulation_noalloc(const double *d_points, int n, double Lx, double Ly,
+                                                double cell_size, int *d_tri, int *d_neighnum, int stride,
+                                                int *out_required_stride, void *stream)
+{
+    if (out_required_stride) *out_required_stride = 0;
+    if (n < 0 || !(Lx > 0) || !(Ly > 0) || !std::isfinite(Lx) || !std::isfinite(Ly) || !std::isfinite(cell_size))
+        return DGT_ERR_INVALID_ARGUMENT;
+    if (n == 0) return DGT_OK;
+    if (n > NA_MAX_POINTS || !d_points || !d_tri || !d_neighnum || stride < 3 || stride > (1 << 16))
+        return DGT_ERR_INVALID_ARGUMENT;
+    // cell grid (same rule as a context: requested edge, no finer than ~4 cells per point)
+    double spacing = std::sqrt(Lx * Ly / n);
+    double a = cell_size > 0 ? cell_size : spacing;
+    double amin = std::sqrt(Lx * Ly / (4.0 * n + 16.0));
+    if (a < amin) a = amin;
+    int xs = std::max(1, (int)std::floor(Lx / a)), ys = std::max(1, (int)std::floor(Ly / a));
+    if ((long long)xs * ys > NA_MAX_CELLS) return DGT_ERR_INVALID_ARGUMENT;
+    SetDesc S;
+    S.Lx = Lx;
+    S.Ly = Ly;
+    S.hLx = 0.5 * Lx;
+    S.hLy = 0.5 * Ly;
+    S.xsize = xs;
+    S.ysize = ys;
+    S.cw = Lx / xs;
+    S.ch = Ly / ys;
+    S.icw = (double)xs / Lx;
+    S.ich = (double)ys / Ly;
+    S.cell_base = 0;
+    S.point_base = 0;
+    S.n = n;
+    S.V = (float)pow2_at_least(std::max(Lx, Ly));
+    S.pad = 0;
+    const int cells = xs * ys;
+
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return DGT_ERR_CUDA;
+    unsigned char *base = nullptr;
+    int rc = scratch_base(dev, &base);
+    if (rc != DGT_OK) return rc;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+    cudaStream_t s = (cudaStream_t)stream;
+
+    SetDesc *d_sets = reinterpret_cast<SetDesc *>(base + OFF_SETS);
+    DevStatus *d_st = reinterpret_cast<DevStatus *>(base + OFF_STATUS);
+    k_noalloc_setup<<<std::min((cells + 1 + 255) / 256, 1024), 256, 0, s>>>(S, d_sets, d_st,
+                                                                          reinterpret_cast<int *>(base + OFF_CCOUNT),
+                                                                          cells + 1);
+    if (cudaGetLastError() != cudaSuccess) return DGT_ERR_CUDA;
+
+    BinArgs b;
+    b.pos = reinterpret_cast<const double2 *>(d_points);
+    b.n = n;
+    b.sets = d_sets;
+    b.set_of = nullptr;
+    b.total_cells = cells;
+    b.ccount = reinterpret_cast<int *>(base + OFF_CCOUNT);
+    b.cstart = reinterpret_cast<int *>(base + OFF_CSTART);
+    b.cell_of = reinterpret_cast<int *>(base + OFF_CELLOF);
+    b.rank = reinterpret_cast<int *>(base + OFF_RANK);
+    b.sidx = reinterpret_cast<int *>(base + OFF_SIDX);
+    b.slot_of = reinterpret_cast<int *>(base + OFF_SLOTOF);
+    b.spos = reinterpret_cast<double2 *>(base + OFF_SPOS);
+    b.block_sums = reinterpret_cast<int *>(base + OFF_BSUM);
+    b.deterministic = 1;
+    if (launch_bin_st(b, d_st, s) != cudaSuccess) return DGT_ERR_CUDA;
+
+    RingArgs r;
+    std::memset(&r, 0, sizeof(r));
+    r.sets = d_sets;
+    r.set_of = nullptr;
+    r.pos = b.pos;
+    r.spos = b.spos;
+    r.sidx = b.sidx;
+    r.slot_of = b.slot_of;
+    r.cstart = b.cstart;
+    r.tri = d_tri;
+    r.nn = d_neighnum;
+    r.stride = stride;
+    r.npoints = n;
+    r.n_items = n;
+    r.slow_list = reinterpret_cast<int *>(base + OFF_SLOWLIST);
+    r.slow_count = &d_st->slow_count;
+    r.st = d_st;
+    if (launch_build(r, MODE_F32, sms, s) != cudaSuccess) return DGT_ERR_CUDA;
+    if (launch_slow(r, base + OFF_SLOWROWS, NA_SLOW_ITEMS, 64, s) != cudaSuccess) return DGT_ERR_CUDA;
+
+    // status into host stack memory (pageable: no pinned buffer is allocated)
+    DevStatus h;
+    if (cudaMemcpyAsync(&h, d_st, sizeof(DevStatus), cudaMemcpyDeviceToHost, s) != cudaSuccess) return DGT_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return DGT_ERR_CUDA;
+    if (h.err_flags & EF_BAD_INPUT) return DGT_ERR_BAD_POINTS;
+    if (h.need_stride > 0) {
+        if (out_required_stride) *out_required_stride = h.need_stride;
+        return DGT_ERR_NEED_RESIZE;
+    }
+    if (h.err_flags & ~EF_MINIMAGE) return DGT_ERR_DEGENERATE;
+    return DGT_OK;
+}

@@ -616,6 +616,7 @@ __global__ void __launch_bounds__(64) k_build_slow(RingArgs A, SlowRow<double> *
     flush_counters(A, ctr, 0, maxr);
 }
 
+static_assert(sizeof(SlowRow<double>) == SLOW_ROW_BYTES, "slow-path row layout");
 size_t slow_scratch_bytes_per_item(int) { return sizeof(SlowRow<double>); }
 
 // ------------------------------------------------------------------ local Delaunay test

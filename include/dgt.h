@@ -142,6 +142,23 @@ int dgt_get_phase_times(dgt_context *ctx, double *out_ms);
 int dgt_displace(dgt_context *ctx, double *d_points, double sigma, unsigned long long seed, unsigned long long step,
                  void *stream);
 
+/* Global triangulation that allocates nothing.  No counterpart in the reference: it is
+ * for callers that must not call cudaMalloc (a host application owns the GPU allocator,
+ * or the memory budget is fixed before this library is loaded).  All scratch lives in one
+ * fixed device array inside the library (about 4.6 MB, present on every GPU that loads the
+ * library until the process exits), so inputs are limited to DGT_NOALLOC_MAX_POINTS points
+ * and a cell grid of DGT_NOALLOC_MAX_CELLS cells (DGT_ERR_INVALID_ARGUMENT beyond that).
+ * Output and precision are those of dgt_global_triangulation (float32 filter) with safety
+ * mode on: the call synchronises `stream`; on DGT_ERR_NEED_RESIZE *out_required_stride
+ * (may be NULL) receives the row stride needed.  All calls share the array: calls whose
+ * work overlaps on a GPU race and must be ordered by the caller.  The first call on each
+ * device looks the array's address up; make it before any stream capture. */
+#define DGT_NOALLOC_MAX_POINTS 65536
+#define DGT_NOALLOC_MAX_CELLS (4 * DGT_NOALLOC_MAX_POINTS + 16)
+int dgt_global_triangulation_noalloc(const double *d_points, int n, double Lx, double Ly, double cell_size,
+                                     int *d_tri, int *d_neighnum, int stride, int *out_required_stride,
+                                     void *stream);
+
 const char *dgt_error_string(int code);
 int dgt_version(void);
 
