@@ -48,9 +48,10 @@ WORKLOADS = {
 # counted.
 BUILD_BYTES_PER_POINT = 16 + 4 + 4 + 24 + 4
 # DRAM bytes per point that ncu measured for k_build (dram__bytes_read.sum +
-# dram__bytes_write.sum over one launch / points), profiles/k_build_fp32_4m.md; None until
-# a capture exists.
-BUILD_DRAM_BYTES_PER_POINT_NCU = None
+# dram__bytes_write.sum of one launch / points) on a 1,048,576-point capture
+# (profiles/k_build_fp32_1m.md); traffic scales with the number of points at fixed density,
+# so the 4M launch is reported as this figure times its points.
+BUILD_DRAM_BYTES_PER_POINT_NCU = 87.2
 FALLBACK_HBM_GBS = 6650.0
 
 
