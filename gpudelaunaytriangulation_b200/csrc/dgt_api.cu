@@ -474,6 +474,8 @@ int dgt_test_and_repair(dgt_context *c, const double *d_points, int *d_tri, int 
     t.sets = c->d_sets.as<SetDesc>();
     t.set_of = c->batch ? c->d_set_of.as<int>() : nullptr;
     t.pos = reinterpret_cast<const double2 *>(d_points);
+    t.sidx = c->sidx.as<int>();
+    t.spos = c->spos.as<double2>();
     t.tri = d_tri;
     t.nn = d_nn;
     t.stride = stride;

@@ -116,6 +116,8 @@ struct TestArgs {
     const SetDesc *sets;
     const int *set_of;
     const double2 *pos;
+    const int *sidx;        // cell-order slot -> point (null: index order)
+    const double2 *spos;    // positions in cell order (used with sidx)
     const int *tri;
     const int *nn;
     int stride;

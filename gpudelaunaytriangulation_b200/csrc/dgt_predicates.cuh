@@ -69,11 +69,20 @@ __device__ __forceinline__ double wrap_off(double c, double p, double L, double 
 // Bound derivation (u = unit roundoff of T; a~, b~ are the T-rounded double offsets):
 //   |n~a - na| <= 4.01u na; |N~ - N| <= 7.2u Nhat (N = na*by - nb*ay etc., Nhat its
 //   permanent); |g~ - g| <= 4.1u ghat, rho = 4.1u ghat / g~.
-//   2c~ = N~/g~ (1+delta):  |2c~ - 2c| (1 - rho) <= 7.2u (Nxhat + Nyhat)/g~ + |2c~| (rho + u)
-//   => E = |c~ - c| <= [3.6u (Nxhat+Nyhat)/g~ + |c~|(rho+u)] / (1-rho), inflated by 1.1.
+//   2c~ = N~ * rcp(g~) (1+delta), |delta| <= 4u with the hardware reciprocal:
+//   |2c~ - 2c| (1 - rho) <= 7.2u (Nxhat + Nyhat)/g~ + |2c~| (rho + 4u)
+//   => E = |c~ - c| <= [3.6u (Nxhat+Nyhat)/g~ + |c~|(rho+4u)] / (1-rho), inflated by 1.1.
 //   Test s~ = fma(dx, 2cx~, fma(dy, 2cy~, -nd~)):
 //   |s~ - s| <= |d|(2E + 2u|c| + 4u|c~|)(1+2u) + 6.1u nd  <= |d| Eb + 8u nd + tiny,
 //   Eb = 2.1E + 8u|c~|.
+// Reciprocal and upper-bounded square root.  float: the hardware approximations (relative
+// error below 2^-22, covered by the 4u terms of the bounds below); double: IEEE operations.
+__device__ __forceinline__ float rcp_approx(float x) { return __fdividef(1.0f, x); }
+__device__ __forceinline__ double rcp_approx(double x) { return 1.0 / x; }
+// sqrt(x) * (1 + tiny) >= sqrt(x); NaN for x == 0 in float (callers treat NaN as undecided)
+__device__ __forceinline__ float sqrt_up(float x) { return x * rsqrtf(x) * 1.00000191f; }
+__device__ __forceinline__ double sqrt_up(double x) { return sqrt(x); }
+
 template <typename T>
 __device__ __forceinline__ typename Prec<T>::T4 make_circ(T ax, T ay, T bx, T by)
 {
@@ -83,15 +92,18 @@ __device__ __forceinline__ typename Prec<T>::T4 make_circ(T ax, T ay, T bx, T by
     T nb = bx * bx + by * by;
     T g = ax * by - ay * bx;
     T gh = fabs(ax * by) + fabs(ay * bx);
+    if (!(g > (T)0) || !((T)4.1 * u * gh <= (T)0.125 * g)) return P::mk4((T)0, (T)0, P::inf(), P::inf());
+    T ig = rcp_approx(g);
+    T rho = (T)4.1 * u * gh * ig * ((T)1 + (T)4 * u);
     T nx = na * by - nb * ay;
     T nxh = na * fabs(by) + nb * fabs(ay);
     T ny = nb * ax - na * bx;
     T nyh = nb * fabs(ax) + na * fabs(bx);
-    T rho = (T)4.1 * u * gh / g;
-    if (!(g > (T)0) || !(rho <= (T)0.125)) return P::mk4((T)0, (T)0, P::inf(), P::inf());
-    T cx2 = nx / g, cy2 = ny / g;
-    T cn = (T)0.5 * sqrt(cx2 * cx2 + cy2 * cy2);
-    T E = ((T)3.6 * u * (nxh + nyh) / g + cn * (rho + u)) / ((T)1 - rho);
+    T cx2 = nx * ig, cy2 = ny * ig;   // relative error <= 4u beyond that of nx, ny
+    T t = cx2 * cx2 + cy2 * cy2;
+    T cn = (t > (T)0) ? (T)0.5 * sqrt_up(t) * ((T)1 + (T)4 * u) : (T)0;
+    // 1 / (1 - rho) <= 1 + 1.2 rho for rho <= 1/8
+    T E = ((T)3.6 * u * (nxh + nyh) * ig * ((T)1 + (T)4 * u) + cn * (rho + (T)4 * u)) * ((T)1 + (T)1.2 * rho);
     E = E * (T)1.1 + P::tiny();
     T eb = (T)2.1 * E + (T)8 * u * cn + P::tiny();
     T rc = cn * ((T)1 + (T)16 * u) + (T)2 * E;   // |c| + |c~ - c| <= |c~| + 2E

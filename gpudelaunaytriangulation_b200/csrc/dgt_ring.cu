@@ -81,10 +81,10 @@ __device__ __forceinline__ int popc_(unsigned long long x) { return __popcll(x);
 __device__ __forceinline__ int ffs_(unsigned int x) { return __ffs(x); }
 __device__ __forceinline__ int ffs_(unsigned long long x) { return __ffsll(x); }
 
+// i in [-n, 2n): one correction brings it into [0, n)
 __device__ __forceinline__ int wrapi(int i, int n)
 {
-    int r = i % n;
-    return r < 0 ? r + n : r;
+    return i < 0 ? i + n : (i >= n ? i - n : i);
 }
 
 template <typename T>
@@ -242,7 +242,7 @@ struct Builder {
         V2 d = PR::mk2(PR::from64(d64.x), PR::from64(d64.y));
         T nd = d.x * d.x + d.y * d.y;
         if (nd > r2max) return R_OK;
-        T ad = sqrt(nd);
+        T ad = sqrt_up(nd);   // only scales the bound: an upper value is safe
         T kb = (T)8 * PR::u() * nd + PR::tiny();
         Mask mask = 0, open = 0;
         for (int k = 0; k < m; ++k) {
@@ -647,10 +647,13 @@ __global__ void __launch_bounds__(256) k_test(TestArgs A)
 {
     unsigned long long flagged = 0;
     for (int base = blockIdx.x * blockDim.x; base < A.n; base += gridDim.x * blockDim.x) {
-        int i = base + threadIdx.x;
+        // points taken in cell order (slot t -> point sidx[t]): the queue a warp appends is a
+        // compact patch of cells, which keeps the repair rounds spatially coherent
+        const int t = base + threadIdx.x;
+        const int i = (t < A.n && A.sidx) ? A.sidx[t] : t;
         int q[TEST_MAX_QUEUE];
         int nq = 0;
-        if (i < A.n) {
+        if (t < A.n) {
             int m = A.nn[i];
             bool bad = (m < 3 || m > A.stride);
             const int *row = A.tri + (size_t)i * A.stride;
@@ -664,7 +667,7 @@ __global__ void __launch_bounds__(256) k_test(TestArgs A)
             }
             if (!bad) {
                 const SetDesc S = A.sets[A.set_of ? A.set_of[i] : 0];
-                double2 p = A.pos[i];
+                double2 p = A.sidx ? A.spos[t] : A.pos[i];
                 double2 q0 = __ldg(&A.pos[row[0]]), ql = __ldg(&A.pos[row[m - 1]]);
                 double2 o0 = make_double2(wrap_off(q0.x, p.x, S.Lx, S.hLx), wrap_off(q0.y, p.y, S.Ly, S.hLy));
                 double2 prev = make_double2(wrap_off(ql.x, p.x, S.Lx, S.hLx), wrap_off(ql.y, p.y, S.Ly, S.hLy));
