@@ -225,6 +225,75 @@ def run_reference(args):
     return 0
 
 
+# compulsory bytes per point of one repair step (bin 16+8, ring + lengths 28, positions 16,
+# cell-order index 4, CSR 8 at one cell per point) plus 48 B per rebuilt point
+REPAIR_BYTES_PER_POINT = 80
+REPAIR_BYTES_PER_REBUILT = 48
+
+
+def ensemble_md_measure(dev, num_sets=256, lo=1000, hi=65536, sigma=0.01, steps=100, graph_steps=10, rounds=4,
+                        seed=7):
+    """Batched ensemble: num_sets independent periodic sets (sizes log-uniform in [lo, hi],
+    unit density) triangulated by one launch sequence, then `steps` MD steps (device
+    displacement sigma + test-and-repair with `rounds` rounds) replayed from a CUDA graph of
+    `graph_steps` steps."""
+    import torch
+
+    from gpudelaunaytriangulation_b200.delaunay import DelaunayBatch
+
+    pts, sizes, boxes = W.ensemble(num_sets, lo, hi, seed=seed)
+    n = len(pts)
+    b = DelaunayBatch(sizes, boxes, 16, 1.0)
+    b.setTiming(True)
+    P = torch.from_numpy(pts).to(dev)
+    P0 = P.clone()
+    tri = torch.zeros(16 * n, dtype=torch.int32, device=dev)
+    nn = torch.zeros(n, dtype=torch.int32, device=dev)
+    for _ in range(3):
+        P.copy_(P0)
+        b.globalDelaunayTriangulation(P, tri, nn)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    b.globalDelaunayTriangulation(P, tri, nn)
+    e1.record()
+    torch.cuda.synchronize()
+    build_ms = e0.elapsed_time(e1)
+    stream = torch.cuda.Stream(device=dev)
+    stream.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(stream):
+        g = b.mdGraph(P, tri, nn, sigma, seed=seed + 1, steps=graph_steps, rounds=rounds, stream=stream)
+        g.launch(stream)   # warm-up replay
+        b.clearFlags(stream)
+        stream.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(steps // graph_steps):
+            g.launch(stream)
+        f1.record(stream)
+        stream.synchronize()
+    md_ms = f0.elapsed_time(f1) / ((steps // graph_steps) * graph_steps)
+    st = b.stats()
+    g.close()
+    # one more MD step outside the graph for the repaired fraction
+    with torch.cuda.stream(stream):
+        b.mdStep(P, tri, nn, sigma, seed=seed + 2, rounds=rounds, stream=stream)
+        stream.synchronize()
+    rep = b.stats()
+    f = rep["repaired"] / n
+    peak, kind = measured_peaks()
+    step_bytes = n * (REPAIR_BYTES_PER_POINT + REPAIR_BYTES_PER_REBUILT * f)
+    achieved = step_bytes / (md_ms / 1e3) / 1e9
+    b.close()
+    return {"sets": num_sets, "points": n, "steps": (steps // graph_steps) * graph_steps, "sigma": sigma,
+            "graph_steps": graph_steps, "rounds": rounds,
+            "build_ms": build_ms, "build_mpts": n / (build_ms / 1e3) / 1e6,
+            "md_ms_per_step": md_ms, "md_mpts": n / (md_ms / 1e3) / 1e6,
+            "repaired_fraction": f, "sticky_flags": st["sticky_flags"],
+            "repair_roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                                "frac": achieved / peak, "bytes_per_point": REPAIR_BYTES_PER_POINT
+                                + REPAIR_BYTES_PER_REBUILT * f, "peak_source": f"{kind} hbm_gbs"}}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -350,6 +419,10 @@ def run_ours(args):
                "h2d_bytes_per_step": 2 * P0.numel() * 8,
                "d2h_bytes_per_step": 2 * (tri.numel() + nn.numel()) * 4, "ms_per_step": ems}
 
+    ens = None
+    if not args.no_ensemble:
+        ens = ensemble_md_measure(dev)
+
     peak, peak_kind = measured_peaks()
     avg_build_s = (sum(build_ms) / len(build_ms)) / 1e3
     bytes_launch = n * BUILD_BYTES_PER_POINT
@@ -388,6 +461,7 @@ def run_ours(args):
                      "exact_points": chk_b["exact_points"] + chk_r["exact_points"],
                      "tests": chk_b["tests"] + chk_r["tests"]},
         "mismatches": chk_b["mismatches"] + chk_r["mismatches"],
+        "ensemble_md": ens,
     }
     if rank == 0:
         print(json.dumps(out))
@@ -407,6 +481,7 @@ def main():
     ap.add_argument("--n", type=int, default=0, help="override the point count (box side sqrt(n))")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble MD measurement")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

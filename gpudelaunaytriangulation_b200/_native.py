@@ -30,8 +30,10 @@ EXPORTED = [
     "dgt_update_list", "dgt_set_cell_size", "dgt_set_box", "dgt_set_safety_mode", "dgt_set_precision",
     "dgt_set_check_mode", "dgt_resize", "dgt_get_max_size", "dgt_get_num_points", "dgt_restride",
     "dgt_get_stats", "dgt_displace", "dgt_error_string", "dgt_version", "dgt_set_timing",
-    "dgt_get_phase_times", "dgt_global_triangulation_noalloc",
+    "dgt_get_phase_times", "dgt_global_triangulation_noalloc", "dgt_md_step", "dgt_md_graph_create",
+    "dgt_md_graph_launch", "dgt_md_graph_destroy", "dgt_clear_flags",
 ]
+STEP_AUTO = 0xFFFFFFFFFFFFFFFF
 NOALLOC_MAX_POINTS = 65536
 PHASES = ["bin", "build", "slow", "test", "repair"]
 
@@ -53,10 +55,14 @@ class Stats(ctypes.Structure):
         ("max_ring", ctypes.c_int),
         ("error_flags", ctypes.c_int),
         ("launches", ctypes.c_int),
+        ("sticky_flags", ctypes.c_int),
+        ("reserved", ctypes.c_int),
+        ("repair_calls", ctypes.c_longlong),
+        ("md_step", ctypes.c_longlong),
     ]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
 class DgtError(RuntimeError):
@@ -112,6 +118,13 @@ def lib() -> ctypes.CDLL:
     L.dgt_version.restype = ctypes.c_int
     L.dgt_set_timing.argtypes = [vp, ctypes.c_int]
     L.dgt_get_phase_times.argtypes = [vp, P_D]
+    L.dgt_md_step.argtypes = [vp, vp, vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_ulonglong, ctypes.c_int, vp]
+    L.dgt_md_graph_create.argtypes = [vp, vp, vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_ulonglong,
+                                      ctypes.c_int, ctypes.c_int, vp, ctypes.POINTER(vp)]
+    L.dgt_md_graph_launch.argtypes = [vp, vp]
+    L.dgt_md_graph_destroy.argtypes = [vp]
+    L.dgt_md_graph_destroy.restype = None
+    L.dgt_clear_flags.argtypes = [vp, vp]
     L.dgt_global_triangulation_noalloc.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                                    ctypes.c_double, vp, vp, ctypes.c_int, P_I, vp]
     _lib = L

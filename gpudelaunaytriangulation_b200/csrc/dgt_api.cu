@@ -51,6 +51,7 @@ struct DevBuf {
 constexpr int SLOW_ITEMS = 2048;    // concurrent exact / large-ring items (scratch rows)
 constexpr int FIRST_ROUNDS = 3;     // repair rounds launched before the first host check
 constexpr int NEXT_ROUNDS = 2;      // rounds per later batch (each kernel exits at once on an empty list)
+constexpr int ASYNC_ROUNDS = 6;     // rounds of an unsynchronised call (convergence flagged on the device)
 
 }  // namespace
 
@@ -69,9 +70,8 @@ struct dgt_context {
     int deterministic = 1;
     std::vector<SetDesc> sets;
     int total_cells = 0;
-    int epoch = 0;
     DevBuf d_sets, d_set_of, ccount, cstart, cell_of, rank, sidx, slot_of, spos, bsum, mark, list0, list1,
-        slow_list, slow_scratch, st;
+        slow_list, slow_scratch, st, ctl;
     DevStatus *h_st = nullptr;
     cudaStream_t last_stream = nullptr;
     bool stats_valid = false;
@@ -208,11 +208,13 @@ int alloc_all(dgt_context *c)
     DGT_TRY(c->list1.ensure(sizeof(int) * n));
     DGT_TRY(c->slow_list.ensure(sizeof(int) * n));
     DGT_TRY(c->slow_scratch.ensure(slow_scratch_bytes_per_item(64) * SLOW_ITEMS));
-    bool fresh_mark = c->mark.bytes < sizeof(int) * (size_t)n;
+    bool fresh_mark = c->mark.bytes < sizeof(int) * (size_t)n || !c->ctl.p;
     DGT_TRY(c->mark.ensure(sizeof(int) * n));
+    DGT_TRY(c->ctl.ensure(sizeof(DevCtl)));
     if (fresh_mark) {
+        // marks and the epoch counter start together at zero
         DGT_TRY(cudaMemset(c->mark.p, 0, sizeof(int) * n));
-        c->epoch = 0;
+        DGT_TRY(cudaMemset(c->ctl.p, 0, sizeof(DevCtl)));
     }
     DGT_TRY(c->st.ensure(sizeof(DevStatus)));
     if (!c->h_st) DGT_TRY(cudaMallocHost(&c->h_st, sizeof(DevStatus)));
@@ -326,6 +328,7 @@ int conclude(dgt_context *c, cudaStream_t s, bool repair_pending)
         c->max_size = std::max(c->max_size, d.need_stride);
         return DGT_ERR_NEED_RESIZE;
     }
+    if (d.err_flags & EF_NOT_CONVERGED) return DGT_ERR_NOT_CONVERGED;
     if (d.err_flags & ~EF_MINIMAGE) return DGT_ERR_DEGENERATE;
     if (repair_pending) return DGT_ERR_NOT_CONVERGED;
     return DGT_OK;
@@ -416,7 +419,7 @@ void dgt_destroy(dgt_context *c)
     if (!c) return;
     DevBuf *bufs[] = { &c->d_sets, &c->d_set_of, &c->ccount, &c->cstart, &c->cell_of, &c->rank, &c->sidx,
                        &c->slot_of, &c->spos, &c->bsum, &c->mark, &c->list0, &c->list1, &c->slow_list,
-                       &c->slow_scratch, &c->st };
+                       &c->slow_scratch, &c->st, &c->ctl };
     for (DevBuf *b : bufs) b->release();
     if (c->h_st) cudaFreeHost(c->h_st);
     for (int p = 0; p < DGT_NUM_PHASES; ++p)
@@ -454,21 +457,27 @@ int dgt_global_triangulation(dgt_context *c, const double *d_points, int *d_tri,
         PhaseTimer t(c, DGT_PHASE_SLOW, s);
         DGT_TRY(run_slow(c, a, s));
     }
+    c->launches += 1;
+    DGT_TRY(launch_call_end(c->ctl.as<DevCtl>(), c->st.as<DevStatus>(), 0, s));
     if (!c->safety) return DGT_OK;
     return conclude(c, s, false);
 }
 
-int dgt_test_and_repair(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, int stride, void *stream)
+}  // extern "C"
+
+namespace {
+
+// Test-and-repair on the context's stream.  fixed_rounds == 0: rounds are launched in
+// batches and the host stops once a list is empty (needs a synchronisation per batch);
+// fixed_rounds > 0: exactly that many rounds, no host synchronisation (graph capture),
+// an unfinished queue sets DGT_FLAG_NOT_CONVERGED in the device flags.
+int repair_impl(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, int stride, cudaStream_t s,
+                int fixed_rounds, bool conclude_now)
 {
-    if (!c) return DGT_ERR_INVALID_ARGUMENT;
-    if (c->n == 0) return DGT_OK;
-    if (!d_points || !d_tri || !d_nn || !valid_stride(stride)) return DGT_ERR_INVALID_ARGUMENT;
-    cudaStream_t s = (cudaStream_t)stream;
-    begin_call(c, s);
     DevStatus *dst = c->st.as<DevStatus>();
+    DevCtl *ctl = c->ctl.as<DevCtl>();
     DGT_TRY(cudaMemsetAsync(c->st.p, 0, sizeof(DevStatus), s));
     DGT_TRY(run_bin(c, d_points, s));
-    const int base = c->epoch + 1;
     int *lists[2] = { c->list0.as<int>(), c->list1.as<int>() };
     TestArgs t;
     t.sets = c->d_sets.as<SetDesc>();
@@ -481,7 +490,7 @@ int dgt_test_and_repair(dgt_context *c, const double *d_points, int *d_tri, int 
     t.stride = stride;
     t.n = c->n;
     t.mark = c->mark.as<int>();
-    t.epoch_base = base;
+    t.epoch_ptr = &ctl->epoch;
     t.list = lists[0];
     t.list_count = &dst->list_count[0];
     t.st = dst;
@@ -494,8 +503,8 @@ int dgt_test_and_repair(dgt_context *c, const double *d_points, int *d_tri, int 
     int round = 0;
     bool pending = false;
     for (;;) {
-        // launch a batch of rounds; each kernel reads its item count on the device
-        int batch = round == 0 ? FIRST_ROUNDS : NEXT_ROUNDS;
+        // a batch of rounds; each kernel reads its item count on the device
+        int batch = fixed_rounds > 0 ? fixed_rounds : (round == 0 ? FIRST_ROUNDS : NEXT_ROUNDS);
         for (int b = 0; b < batch; ++b, ++round) {
             int cur = round & 1, nxt = cur ^ 1;
             DGT_TRY(cudaMemsetAsync(&dst->list_count[nxt], 0, sizeof(int), s));
@@ -505,18 +514,14 @@ int dgt_test_and_repair(dgt_context *c, const double *d_points, int *d_tri, int 
             a.worklist_count = &dst->list_count[cur];
             a.n_items = c->n;
             a.repair = 1;
-            a.epoch_base = base;
-            a.epoch = base + round;
+            a.epoch_ptr = &ctl->epoch;
+            a.round = round;
             a.next_list = lists[nxt];
             a.next_count = &dst->list_count[nxt];
             DGT_TRY(run_build(c, a, s));
             DGT_TRY(run_slow(c, a, s));
         }
-        if (!c->safety) {
-            c->epoch = base + round;
-            phase_end(c, DGT_PHASE_REPAIR, s);
-            return DGT_OK;
-        }
+        if (fixed_rounds > 0) break;
         int left = 0;
         DGT_TRY(cudaMemcpyAsync(&left, &dst->list_count[round & 1], sizeof(int), cudaMemcpyDeviceToHost, s));
         DGT_TRY(cudaStreamSynchronize(s));
@@ -526,9 +531,26 @@ int dgt_test_and_repair(dgt_context *c, const double *d_points, int *d_tri, int 
             break;
         }
     }
-    c->epoch = base + round;
     phase_end(c, DGT_PHASE_REPAIR, s);
+    c->launches += 1;
+    DGT_TRY(launch_call_end(ctl, dst, round, s));
+    if (!conclude_now) return DGT_OK;
     return conclude(c, s, pending);
+}
+
+}  // namespace
+
+extern "C" {
+
+int dgt_test_and_repair(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, int stride, void *stream)
+{
+    if (!c) return DGT_ERR_INVALID_ARGUMENT;
+    if (c->n == 0) return DGT_OK;
+    if (!d_points || !d_tri || !d_nn || !valid_stride(stride)) return DGT_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = (cudaStream_t)stream;
+    begin_call(c, s);
+    if (c->safety) return repair_impl(c, d_points, d_tri, d_nn, stride, s, 0, true);
+    return repair_impl(c, d_points, d_tri, d_nn, stride, s, ASYNC_ROUNDS, false);
 }
 
 int dgt_set_cell_size(dgt_context *c, double cell_size)
@@ -607,6 +629,11 @@ int dgt_get_stats(dgt_context *c, dgt_stats *out)
     }
     to_stats(*c->h_st, out);
     out->launches = c->launches;
+    DevCtl ctl;
+    DGT_TRY(cudaMemcpy(&ctl, c->ctl.p, sizeof(DevCtl), cudaMemcpyDeviceToHost));
+    out->sticky_flags = ctl.sticky;
+    out->repair_calls = (long long)ctl.calls;
+    out->md_step = (long long)ctl.step;
     return DGT_OK;
 }
 
@@ -640,8 +667,89 @@ int dgt_displace(dgt_context *c, double *d_points, double sigma, unsigned long l
                  void *stream)
 {
     if (!c || (c->n > 0 && !d_points) || !(sigma >= 0) || !std::isfinite(sigma)) return DGT_ERR_INVALID_ARGUMENT;
+    unsigned long long *step_ptr = step == DGT_STEP_AUTO ? &c->ctl.as<DevCtl>()->step : nullptr;
     DGT_TRY(launch_displace(reinterpret_cast<double2 *>(d_points), c->n, c->d_sets.as<SetDesc>(),
-                            c->batch ? c->d_set_of.as<int>() : nullptr, sigma, seed, step, (cudaStream_t)stream));
+                            c->batch ? c->d_set_of.as<int>() : nullptr, sigma, seed, step, step_ptr,
+                            (cudaStream_t)stream));
+    return DGT_OK;
+}
+
+int dgt_md_step(dgt_context *c, double *d_points, int *d_tri, int *d_nn, int stride, double sigma,
+                unsigned long long seed, int rounds, void *stream)
+{
+    if (!c || rounds < 1 || rounds > 64) return DGT_ERR_INVALID_ARGUMENT;
+    if (c->n == 0) return DGT_OK;
+    if (!d_points || !d_tri || !d_nn || !valid_stride(stride)) return DGT_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = (cudaStream_t)stream;
+    int r = dgt_displace(c, d_points, sigma, seed, DGT_STEP_AUTO, stream);
+    if (r != DGT_OK) return r;
+    begin_call(c, s);
+    c->launches += 2;
+    return repair_impl(c, d_points, d_tri, d_nn, stride, s, rounds, false);
+}
+
+struct dgt_graph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int steps = 0;
+};
+
+int dgt_md_graph_create(dgt_context *c, double *d_points, int *d_tri, int *d_nn, int stride, double sigma,
+                        unsigned long long seed, int steps, int rounds, void *stream, dgt_graph **out)
+{
+    if (!out) return DGT_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (!c || !stream || steps < 1 || steps > 100000) return DGT_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = (cudaStream_t)stream;
+    const bool timing = c->timing;
+    c->timing = false;   // no event records inside the graph
+    DGT_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    int r = DGT_OK;
+    for (int k = 0; k < steps && r == DGT_OK; ++k) r = dgt_md_step(c, d_points, d_tri, d_nn, stride, sigma, seed, rounds, stream);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s, &g);
+    c->timing = timing;
+    if (r != DGT_OK) {
+        if (g) cudaGraphDestroy(g);
+        return r;
+    }
+    if (e != cudaSuccess) return cuda_status(e);
+    dgt_graph *G = new (std::nothrow) dgt_graph();
+    if (!G) {
+        cudaGraphDestroy(g);
+        return DGT_ERR_OUT_OF_MEMORY;
+    }
+    G->graph = g;
+    G->steps = steps;
+    e = cudaGraphInstantiate(&G->exec, g, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        delete G;
+        return cuda_status(e);
+    }
+    *out = G;
+    return DGT_OK;
+}
+
+int dgt_md_graph_launch(dgt_graph *g, void *stream)
+{
+    if (!g || !g->exec) return DGT_ERR_INVALID_ARGUMENT;
+    DGT_TRY(cudaGraphLaunch(g->exec, (cudaStream_t)stream));
+    return DGT_OK;
+}
+
+void dgt_md_graph_destroy(dgt_graph *g)
+{
+    if (!g) return;
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+}
+
+int dgt_clear_flags(dgt_context *c, void *stream)
+{
+    if (!c) return DGT_ERR_INVALID_ARGUMENT;
+    DGT_TRY(cudaMemsetAsync(&c->ctl.as<DevCtl>()->sticky, 0, sizeof(int), (cudaStream_t)stream));
     return DGT_OK;
 }
 

@@ -197,10 +197,12 @@ __device__ __forceinline__ double wrap_coord(double x, double L)
 }
 
 __global__ void __launch_bounds__(256) k_displace(double2 *pos, int n, const SetDesc *sets, const int *set_of,
-                                                  double sigma, unsigned long long seed, unsigned long long step)
+                                                  double sigma, unsigned long long seed, unsigned long long step,
+                                                  const unsigned long long *step_ptr)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    if (step_ptr) step = *step_ptr;
     const SetDesc &S = sets[set_of ? set_of[i] : 0];
     unsigned long long h = smix(seed ^ smix(step * 0x100000001B3ULL + (unsigned long long)i));
     unsigned long long h2 = smix(h);
@@ -215,11 +217,15 @@ __global__ void __launch_bounds__(256) k_displace(double2 *pos, int n, const Set
     pos[i] = p;
 }
 
+__global__ void k_advance_step(unsigned long long *step_ptr) { *step_ptr += 1; }
+
 cudaError_t launch_displace(double2 *pos, int n, const SetDesc *sets, const int *set_of, double sigma,
-                            unsigned long long seed, unsigned long long step, cudaStream_t s)
+                            unsigned long long seed, unsigned long long step, unsigned long long *step_ptr,
+                            cudaStream_t s)
 {
     if (n <= 0) return cudaSuccess;
-    k_displace<<<(n + 255) / 256, 256, 0, s>>>(pos, n, sets, set_of, sigma, seed, step);
+    k_displace<<<(n + 255) / 256, 256, 0, s>>>(pos, n, sets, set_of, sigma, seed, step, step_ptr);
+    if (step_ptr) k_advance_step<<<1, 1, 0, s>>>(step_ptr);
     return cudaGetLastError();
 }
 

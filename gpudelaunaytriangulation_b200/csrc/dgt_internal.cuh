@@ -62,6 +62,16 @@ enum : int {
     // warning, not an error: a certified circle reached past half the box, where minimum-
     // image offsets stop being unique (the box is too small for that point's Delaunay star)
     EF_MINIMAGE = 32,
+    EF_NOT_CONVERGED = 64, // repair rounds ran out with points still queued
+};
+
+// device-resident control block of a context: everything that changes from call to call
+// lives here so a captured CUDA graph replays correctly
+struct DevCtl {
+    int epoch;                  // last repair epoch used (marks >= epoch+1 belong to the next call)
+    int sticky;                 // error flags of every call since the last reset
+    unsigned long long step;    // displacement step counter (dgt_displace with DGT_STEP_AUTO)
+    unsigned long long calls;   // test-and-repair calls completed
 };
 
 enum : int { MODE_F32 = 0, MODE_F64 = 1 };
@@ -98,11 +108,12 @@ struct RingArgs {
     const int *worklist;
     const int *worklist_count;  // device count (used when worklist != null)
     int n_items;
-    // repair bookkeeping
+    // repair bookkeeping: this call's base epoch is *epoch_ptr + 1, round r's items carry
+    // mark base + r and queue the next round with base + r + 1
     int repair;        // 1: rebuild listed points and propagate consistency checks
     int *mark;
-    int epoch_base;
-    int epoch;         // mark value of the items of this round; next round uses epoch + 1
+    const int *epoch_ptr;
+    int round;
     int *next_list;
     int *next_count;
     // deferred items for the exact / large-capacity kernel
@@ -123,7 +134,7 @@ struct TestArgs {
     int stride;
     int n;
     int *mark;
-    int epoch_base;
+    const int *epoch_ptr;   // this call's base epoch is *epoch_ptr + 1
     int *list;
     int *list_count;
     DevStatus *st;
@@ -138,8 +149,13 @@ cudaError_t launch_slow(const RingArgs &a, void *scratch, int scratch_items, int
 cudaError_t launch_test(const TestArgs &a, cudaStream_t s);
 cudaError_t launch_restride(const int *src, int old_stride, int *dst, int new_stride, const int *nn, int n,
                             cudaStream_t s);
+// step_ptr != null: the step comes from (and is advanced in) device memory
 cudaError_t launch_displace(double2 *pos, int n, const SetDesc *sets, const int *set_of, double sigma,
-                            unsigned long long seed, unsigned long long step, cudaStream_t s);
+                            unsigned long long seed, unsigned long long step, unsigned long long *step_ptr,
+                            cudaStream_t s);
+// end of a test-and-repair call: fold flags into the sticky word, check convergence,
+// advance the epoch by rounds + 1
+cudaError_t launch_call_end(DevCtl *ctl, DevStatus *st, int rounds, cudaStream_t s);
 size_t slow_scratch_bytes_per_item(int capacity);
 // bytes of one row of the exact / large-ring path (64 entries of double4 + double2 + int)
 constexpr size_t SLOW_ROW_BYTES = 64 * (sizeof(double4) + sizeof(double2) + sizeof(int));

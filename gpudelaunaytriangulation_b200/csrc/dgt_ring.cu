@@ -435,14 +435,16 @@ struct Builder {
 };
 
 // ------------------------------------------------------------- output + repair bookkeeping
-__device__ __forceinline__ void enqueue_next(const RingArgs &A, int j)
+__device__ __forceinline__ void enqueue_next(const RingArgs &A, int ebase, int ep, int j)
 {
-    if (atomicMax(&A.mark[j], A.epoch + 1) < A.epoch_base) A.next_list[atomicAdd(A.next_count, 1)] = j;
+    if (atomicMax(&A.mark[j], ep + 1) < ebase) A.next_list[atomicAdd(A.next_count, 1)] = j;
 }
 
 template <class Ring>
 __device__ void finish(const RingArgs &A, int pid, Ring &R, int m, int &maxr)
 {
+    const int ebase = A.repair ? *A.epoch_ptr + 1 : 0;
+    const int ep = ebase + A.round;
     maxr = max(maxr, m);
     int *row = A.tri + (size_t)pid * A.stride;
     if (A.repair) {
@@ -455,12 +457,12 @@ __device__ void finish(const RingArgs &A, int pid, Ring &R, int m, int &maxr)
                 int o = row[k];
                 bool kept = false;
                 for (int t = 0; t < m; ++t) kept |= (R.idx(t) == o);
-                if (!kept && o >= 0 && o < A.npoints) enqueue_next(A, o);
+                if (!kept && o >= 0 && o < A.npoints) enqueue_next(A, ebase, ep, o);
             }
         }
         for (int k = 0; k < m; ++k) {
             int nb = R.idx(k);
-            if (A.mark[nb] >= A.epoch_base) continue;
+            if (A.mark[nb] >= ebase) continue;
             int pred = R.idx(k == 0 ? m - 1 : k - 1), succ = R.idx(k + 1 == m ? 0 : k + 1);
             int mn = A.nn[nb];
             bool ok = (mn >= 3 && mn <= A.stride);
@@ -471,7 +473,7 @@ __device__ void finish(const RingArgs &A, int pid, Ring &R, int m, int &maxr)
                     if (rn[t] == pid) pos = t;
                 ok = pos >= 0 && rn[pos == 0 ? mn - 1 : pos - 1] == succ && rn[pos + 1 == mn ? 0 : pos + 1] == pred;
             }
-            if (!ok) enqueue_next(A, nb);
+            if (!ok) enqueue_next(A, ebase, ep, nb);
         }
     }
     if (m > A.stride) {
@@ -534,7 +536,7 @@ __global__ void __launch_bounds__(BLOCK) k_build(RingArgs A)
     const int n = item_count(A);
     if (A.repair && blockIdx.x == 0 && threadIdx.x == 0 && n > 0) {
         atomicAdd(&A.st->repaired, (unsigned long long)n);
-        atomicMax(&A.st->rounds, A.epoch - A.epoch_base + 1);
+        atomicMax(&A.st->rounds, A.round + 1);
     }
     for (int base = blockIdx.x * BLOCK; base < n; base += gridDim.x * BLOCK) {
         // every lane runs the builder (it votes across the warp); lanes past the end idle
@@ -646,6 +648,7 @@ constexpr int TEST_MAX_QUEUE = 24;
 __global__ void __launch_bounds__(256) k_test(TestArgs A)
 {
     unsigned long long flagged = 0;
+    const int ebase = *A.epoch_ptr + 1;
     for (int base = blockIdx.x * blockDim.x; base < A.n; base += gridDim.x * blockDim.x) {
         // points taken in cell order (slot t -> point sidx[t]): the queue a warp appends is a
         // compact patch of cells, which keeps the repair rounds spatially coherent
@@ -700,7 +703,7 @@ __global__ void __launch_bounds__(256) k_test(TestArgs A)
                 if (cross != 1) bad = true;
             }
             if (bad || nf > 0) {
-                if (atomicMax(&A.mark[i], A.epoch_base) < A.epoch_base) q[nq++] = i;
+                if (atomicMax(&A.mark[i], ebase) < ebase) q[nq++] = i;
                 if (!bad) {
                     // a spoke failure: its quadrilateral; more than three failures: the whole fan
                     if (nf <= 3) {
@@ -708,12 +711,12 @@ __global__ void __launch_bounds__(256) k_test(TestArgs A)
                             int k = fail_k[f];
                             int js[3] = { row[k == 0 ? m - 1 : k - 1], row[k], row[k + 1 == m ? 0 : k + 1] };
                             for (int t = 0; t < 3; ++t)
-                                if (nq < TEST_MAX_QUEUE && atomicMax(&A.mark[js[t]], A.epoch_base) < A.epoch_base)
+                                if (nq < TEST_MAX_QUEUE && atomicMax(&A.mark[js[t]], ebase) < ebase)
                                     q[nq++] = js[t];
                         }
                     } else {
                         for (int k = 0; k < m; ++k)
-                            if (nq < TEST_MAX_QUEUE && atomicMax(&A.mark[row[k]], A.epoch_base) < A.epoch_base)
+                            if (nq < TEST_MAX_QUEUE && atomicMax(&A.mark[row[k]], ebase) < ebase)
                                 q[nq++] = row[k];
                     }
                 }
@@ -762,6 +765,26 @@ cudaError_t launch_test(const TestArgs &a, cudaStream_t s)
     if (a.n <= 0) return cudaSuccess;
     int blocks = (a.n + 255) / 256;
     k_test<<<blocks, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+__global__ void k_call_end(DevCtl *ctl, DevStatus *st, int rounds)
+{
+    int f = st->err_flags;
+    if (rounds > 0) {
+        if (st->list_count[rounds & 1] > 0) {
+            f |= EF_NOT_CONVERGED;
+            st->err_flags |= EF_NOT_CONVERGED;
+        }
+        ctl->epoch += rounds + 1;
+        ctl->calls += 1;
+    }
+    ctl->sticky |= f;
+}
+
+cudaError_t launch_call_end(DevCtl *ctl, DevStatus *st, int rounds, cudaStream_t s)
+{
+    k_call_end<<<1, 1, 0, s>>>(ctl, st, rounds);
     return cudaGetLastError();
 }
 

@@ -202,6 +202,31 @@ class DelaunayGPU:
         _nat.check(self._L.dgt_displace(self._h, _ptr(points), float(sigma), int(seed) & (2**64 - 1),
                                      int(step) & (2**64 - 1), _stream_ptr(stream)), "dgt_displace")
 
+    def mdStep(self, points: torch.Tensor, tri: torch.Tensor, nn: torch.Tensor, sigma: float, seed: int,
+               rounds: int = 4, stream=None):
+        """One device-only MD step: Gaussian displacement (device step counter) then
+        test-and-repair with a fixed number of rounds; no host synchronisation."""
+        _check_points(points, self.Ncells)
+        stride = tri.numel() // max(1, self.Ncells)
+        _nat.check(self._L.dgt_md_step(self._h, _ptr(points), _ptr(tri), _ptr(nn), stride, float(sigma),
+                                       int(seed) & (2**64 - 1), int(rounds), _stream_ptr(stream)), "dgt_md_step")
+
+    def mdGraph(self, points: torch.Tensor, tri: torch.Tensor, nn: torch.Tensor, sigma: float, seed: int,
+                steps: int, rounds: int = 4, stream=None) -> "MDGraph":
+        """Capture `steps` MD steps into a CUDA graph (stream must not be the default one)."""
+        _check_points(points, self.Ncells)
+        if stream is None:
+            raise ValueError("graph capture needs a non-default torch.cuda.Stream")
+        stride = tri.numel() // max(1, self.Ncells)
+        g = ctypes.c_void_p()
+        _nat.check(self._L.dgt_md_graph_create(self._h, _ptr(points), _ptr(tri), _ptr(nn), stride, float(sigma),
+                                               int(seed) & (2**64 - 1), int(steps), int(rounds),
+                                               _stream_ptr(stream), ctypes.byref(g)), "dgt_md_graph_create")
+        return MDGraph(self._L, g, steps)
+
+    def clearFlags(self, stream=None):
+        _nat.check(self._L.dgt_clear_flags(self._h, _stream_ptr(stream)), "dgt_clear_flags")
+
     def setTiming(self, on: bool):
         """Record CUDA events around each phase of every call (see phaseTimes)."""
         _nat.check(self._L.dgt_set_timing(self._h, 1 if on else 0), "dgt_set_timing")
@@ -222,6 +247,29 @@ class DelaunayGPU:
         if getattr(self, "_h", None) and self._h.value:
             self._L.dgt_destroy(self._h)
             self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class MDGraph:
+    """An instantiated CUDA graph of MD steps (see DelaunayGPU.mdGraph)."""
+
+    def __init__(self, lib, handle, steps):
+        self._L = lib
+        self._g = handle
+        self.steps = steps
+
+    def launch(self, stream=None):
+        _nat.check(self._L.dgt_md_graph_launch(self._g, _stream_ptr(stream)), "dgt_md_graph_launch")
+
+    def close(self):
+        if self._g and self._g.value:
+            self._L.dgt_md_graph_destroy(self._g)
+            self._g = ctypes.c_void_p()
 
     def __del__(self):
         try:

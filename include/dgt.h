@@ -50,8 +50,12 @@ typedef struct dgt_stats {
     long long cells;           /* grid cells scanned */
     int repair_rounds;         /* test-and-repair: rounds until no ring changed */
     int max_ring;              /* largest ring of the call */
-    int error_flags;           /* DGT_FLAG_* bits */
-    int launches;              /* kernels this library launched in the call */
+    int error_flags;           /* DGT_FLAG_* bits of the last call */
+    int launches;              /* kernels this library launched in the last call */
+    int sticky_flags;          /* DGT_FLAG_* bits of every call since dgt_clear_flags */
+    int reserved;
+    long long repair_calls;    /* test-and-repair calls completed on the device */
+    long long md_step;         /* device step counter used by DGT_STEP_AUTO */
 } dgt_stats;
 
 /* phases timed with CUDA events when timing is on (dgt_set_timing) */
@@ -72,6 +76,7 @@ typedef struct dgt_stats {
    offsets are no longer unique (the reference has the same limit); results for such
    points follow the minimum-image convention */
 #define DGT_FLAG_MINIMUM_IMAGE 32
+#define DGT_FLAG_NOT_CONVERGED 64 /* an unsynchronised repair ran out of rounds with points queued */
 
 /* DelaunayGPU(int N, int maximumNeighborsGuess, double cellSize, PeriodicBoxPtr bx)
  * (src/model/DelaunayGPU.h:25, DelaunayGPU.cpp:11-37).  Rectangular periodic box Lx x Ly.
@@ -138,9 +143,28 @@ int dgt_get_phase_times(dgt_context *ctx, double *out_ms);
 
 /* MD-like helper: every point += sigma * N(0,1) per axis (counter-based normals of
  * (seed, step, index)), wrapped into its box (periodicBoundaries::move,
- * periodicBoundaries.h:181-189). */
+ * periodicBoundaries.h:181-189).  step == DGT_STEP_AUTO takes the step from a counter in
+ * device memory and advances it (so a captured graph draws new noise on every replay). */
+#define DGT_STEP_AUTO 0xFFFFFFFFFFFFFFFFULL
 int dgt_displace(dgt_context *ctx, double *d_points, double sigma, unsigned long long seed, unsigned long long step,
                  void *stream);
+
+/* One MD-like step without any host synchronisation, suitable for stream capture:
+ * dgt_displace(DGT_STEP_AUTO) then test-and-repair with exactly `rounds` repair rounds.
+ * Overflow / unfinished repair show up in dgt_stats.sticky_flags.  No reference
+ * counterpart: the reference's driver moves points on the host (triangulation.cpp:349-364). */
+int dgt_md_step(dgt_context *ctx, double *d_points, int *d_tri, int *d_neighnum, int stride, double sigma,
+                unsigned long long seed, int rounds, void *stream);
+
+/* `steps` MD steps captured into one CUDA graph on `stream` (must not be the legacy default
+ * stream); every dgt_md_graph_launch replays them with fresh noise and fresh repair epochs. */
+typedef struct dgt_graph dgt_graph;
+int dgt_md_graph_create(dgt_context *ctx, double *d_points, int *d_tri, int *d_neighnum, int stride, double sigma,
+                        unsigned long long seed, int steps, int rounds, void *stream, dgt_graph **out);
+int dgt_md_graph_launch(dgt_graph *graph, void *stream);
+void dgt_md_graph_destroy(dgt_graph *graph);
+/* reset dgt_stats.sticky_flags */
+int dgt_clear_flags(dgt_context *ctx, void *stream);
 
 /* Global triangulation that allocates nothing.  No counterpart in the reference: it is
  * for callers that must not call cudaMalloc (a host application owns the GPU allocator,

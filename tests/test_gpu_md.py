@@ -1,0 +1,73 @@
+"""Device-only MD steps on a batched ensemble: displacement + fixed-round repair, directly
+and replayed from a captured CUDA graph; every set's rings must equal a fresh oracle
+triangulation of the displaced points."""
+import numpy as np
+import pytest
+
+from gpudelaunaytriangulation_b200 import workloads as W
+from oracle import oracle as O
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+def check_sets(P, tri, nn, sizes, boxes):
+    cur = P.cpu().numpy()
+    n = nn.numel()
+    t = tri.view(n, -1).cpu().numpy()
+    k = nn.cpu().numpy()
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    for s in range(len(sizes)):
+        lo, hi = off[s], off[s + 1]
+        ref = O.restated_global(cur[lo:hi], boxes[s][0], boxes[s][1], 1.0, 32)
+        ts = t[lo:hi].copy()
+        ts[np.arange(ts.shape[1])[None, :] < k[lo:hi, None]] -= lo
+        assert np.array_equal(k[lo:hi], ref.nn), s
+        assert np.array_equal(O.canonical(ts, k[lo:hi])[:, : t.shape[1]],
+                              O.canonical(ref.tri, ref.nn)[:, : t.shape[1]]), s
+
+
+def setup(num_sets=10, lo=500, hi=8000, seed=21):
+    from gpudelaunaytriangulation_b200.delaunay import DelaunayBatch
+
+    pts, sizes, boxes = W.ensemble(num_sets, lo, hi, seed=seed)
+    b = DelaunayBatch(sizes, boxes, 16, 1.0)
+    P = torch.from_numpy(pts).cuda()
+    tri, nn = b.globalDelaunayTriangulation(P)
+    return b, P, tri, nn, sizes, boxes
+
+
+def test_md_steps_without_graph():
+    b, P, tri, nn, sizes, boxes = setup()
+    for _ in range(3):
+        b.mdStep(P, tri, nn, 0.01, seed=5, rounds=4)
+    torch.cuda.synchronize()
+    st = b.stats()
+    assert st["sticky_flags"] == 0 and st["md_step"] == 3
+    check_sets(P, tri, nn, sizes, boxes)
+
+
+def test_md_graph_replays_fresh_noise_and_matches_oracle():
+    b, P, tri, nn, sizes, boxes = setup(seed=22)
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        g = b.mdGraph(P, tri, nn, 0.01, seed=9, steps=4, rounds=4, stream=stream)
+        before = P.clone()
+        g.launch(stream)
+        stream.synchronize()
+        mid = P.clone()
+        g.launch(stream)
+        stream.synchronize()
+    assert not torch.equal(before, mid) and not torch.equal(mid, P)
+    st = b.stats()
+    assert st["sticky_flags"] == 0 and st["md_step"] == 8 and st["repair_calls"] == 8
+    check_sets(P, tri, nn, sizes, boxes)
+    g.close()
+
+
+def test_unfinished_repair_is_flagged_not_hidden():
+    # one round only and a large move: the queue cannot drain, the device flag must say so
+    b, P, tri, nn, sizes, boxes = setup(num_sets=3, lo=2000, hi=4000, seed=23)
+    b.mdStep(P, tri, nn, 0.3, seed=1, rounds=1)
+    torch.cuda.synchronize()
+    assert b.stats()["sticky_flags"] & 64
