@@ -32,6 +32,7 @@ if ROOT not in sys.path:
 import numpy as np  # noqa: E402
 
 from gpudelaunaytriangulation_b200 import workloads as W  # noqa: E402
+from gpudelaunaytriangulation_b200.replicas import ReplicaGroup, replica_seed  # noqa: E402
 
 METRIC = "Mpoints/s full build + repair on 1 B200, FP32-filter vs FP64 plain, 0 mismatches"
 UNIT = "Mpoints/s"
@@ -249,6 +250,7 @@ def ensemble_md_measure(dev, num_sets=256, lo=1000, hi=65536, sigma=0.01, steps=
     P0 = P.clone()
     tri = torch.zeros(16 * n, dtype=torch.int32, device=dev)
     nn = torch.zeros(n, dtype=torch.int32, device=dev)
+    tune = b.autotune(P, tri, nn)   # cell size (relative to each set's spacing) and kernel shape
     for _ in range(3):
         P.copy_(P0)
         b.globalDelaunayTriangulation(P, tri, nn)
@@ -288,10 +290,76 @@ def ensemble_md_measure(dev, num_sets=256, lo=1000, hi=65536, sigma=0.01, steps=
             "graph_steps": graph_steps, "rounds": rounds,
             "build_ms": build_ms, "build_mpts": n / (build_ms / 1e3) / 1e6,
             "md_ms_per_step": md_ms, "md_mpts": n / (md_ms / 1e3) / 1e6,
-            "repaired_fraction": f, "sticky_flags": st["sticky_flags"],
+            "repaired_fraction": f, "sticky_flags": st["sticky_flags"], "tuning": tune,
             "repair_roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                                 "frac": achieved / peak, "bytes_per_point": REPAIR_BYTES_PER_POINT
                                 + REPAIR_BYTES_PER_REBUILT * f, "peak_source": f"{kind} hbm_gbs"}}
+
+
+def _timed_call(fn, stream=None):
+    import torch
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def configs_measure(dev):
+    """The other workload families, each measured once (not the headline): 1M points with 20
+    float64 repair steps; 1M-site jittered triangular lattice and 1M-point 64-cluster Gaussian
+    mixture (float32 filter, autotuned settings, check mode for mismatches)."""
+    import torch
+
+    from gpudelaunaytriangulation_b200.delaunay import DelaunayGPU
+
+    out = {}
+    # 1,000,000 uniform points, L = 1000: build, then 20 steps of displacement + repair, float64
+    n, L = 1_000_000, 1000.0
+    P = torch.from_numpy(W.uniform_points(n, L, 31)).to(dev)
+    d = DelaunayGPU(n, 16, 1.0, (L, L))
+    d.setPrecision(False)
+    tri = torch.zeros(16 * n, dtype=torch.int32, device=dev)
+    nn = torch.zeros(n, dtype=torch.int32, device=dev)
+    d.globalDelaunayTriangulation(P, tri, nn)
+    b_ms = _timed_call(lambda: d.globalDelaunayTriangulation(P, tri, nn))
+    rep = []
+
+    def steps():
+        for k in range(20):
+            d.displace(P, 0.02, seed=32, step=k)
+            d.testAndRepairDelaunayTriangulation(P, tri, nn)
+            rep.append(d.stats()["repaired"])
+
+    s_ms = _timed_call(steps) / 20
+    out["uniform_1m_fp64_20_steps"] = {"points": n, "build_ms": b_ms, "repair_step_ms": s_ms,
+                                       "build_mpts": n / b_ms / 1e3, "repair_step_mpts": n / s_ms / 1e3,
+                                       "repaired_per_step": float(np.mean(rep)),
+                                       "sum_ring_sizes_is_6n": int(nn.sum().item()) == 6 * n}
+    d.close()
+    # near-degenerate lattice and clustered mixture, float32 filter, autotuned
+    lat, Lx, Ly = W.triangular_lattice(1024, 1024, 1.0, 1e-4, seed=3)
+    mix, Lm = W.gaussian_mixture(1 << 20, components=64, sigma=2.0, L=1024.0, seed=5)
+    for name, pts, bx, by in (("lattice_1m_fp32", lat, Lx, Ly), ("mixture_1m_fp32", mix, Lm, Lm)):
+        n = len(pts)
+        P = torch.from_numpy(pts).to(dev)
+        d = DelaunayGPU(n, 16, 0.0, (bx, by))
+        tri = torch.zeros(16 * n, dtype=torch.int32, device=dev)
+        nn = torch.zeros(n, dtype=torch.int32, device=dev)
+        tune = d.autotune(P, tri, nn)
+        b_ms = _timed_call(lambda: d.globalDelaunayTriangulation(P, tri, nn))
+        d.setCheckMode(True)
+        d.globalDelaunayTriangulation(P, tri, nn)
+        st = d.stats()
+        out[name] = {"points": n, "build_ms": b_ms, "build_mpts": n / b_ms / 1e3, "tuning": tune,
+                     "fp32_undecided_frac": st["fp32_undecided"] / max(1, st["tests"]),
+                     "fp64_undecided": st["fp64_undecided"], "exact_points": st["exact_points"],
+                     "mismatches": st["mismatches"], "flags": st["error_flags"], "max_ring": st["max_ring"],
+                     "sum_ring_sizes_is_6n": int(nn[: n].sum().item()) == 6 * n}
+        d.close()
+    return out
 
 
 def run_ours(args):
@@ -309,7 +377,8 @@ def run_ours(args):
     n, L, sigma, cell, maxn = WORKLOADS[args.workload]
     if args.n:
         n, L = args.n, float(np.sqrt(args.n))
-    seed = 2026 + 7919 * rank
+    group = ReplicaGroup(world, rank, dev)
+    seed = replica_seed(2026, rank)
     p0 = W.uniform_points(n, L, seed)
     p1 = W.displace(p0, sigma, L, L, seed + 1)
     P0 = torch.from_numpy(p0).to(dev)
@@ -320,16 +389,8 @@ def run_ours(args):
     d.setTiming(True)
     stream = torch.cuda.current_stream()
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier = group.barrier
+    max_over_ranks = group.max_over_ranks
 
     def timed(precision_fp32: bool, steps: int, warmup: int, sample_clocks=False):
         d.setPrecision(precision_fp32)
@@ -364,7 +425,7 @@ def run_ours(args):
 
     # headline: float32 filter
     ms, build_ms, launches, repaired, rounds, clocks = timed(True, args.steps, args.warmup, sample_clocks=True)
-    value = world * n / (ms / 1e3) / 1e6
+    value, _ = group.throughput(n, ms)
     # phase split of one extra step (outside the timed region)
     d.globalDelaunayTriangulation(P0, tri, nn)
     ph_build = d.phaseTimes()
@@ -422,6 +483,9 @@ def run_ours(args):
     ens = None
     if not args.no_ensemble:
         ens = ensemble_md_measure(dev)
+    other = None
+    if not args.no_configs and world == 1:
+        other = configs_measure(dev)
 
     peak, peak_kind = measured_peaks()
     avg_build_s = (sum(build_ms) / len(build_ms)) / 1e3
@@ -462,6 +526,7 @@ def run_ours(args):
                      "tests": chk_b["tests"] + chk_r["tests"]},
         "mismatches": chk_b["mismatches"] + chk_r["mismatches"],
         "ensemble_md": ens,
+        "configs": other,
     }
     if rank == 0:
         print(json.dumps(out))
@@ -482,6 +547,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble MD measurement")
+    ap.add_argument("--no-configs", action="store_true", help="skip the other workload families")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -31,7 +31,8 @@ EXPORTED = [
     "dgt_set_check_mode", "dgt_resize", "dgt_get_max_size", "dgt_get_num_points", "dgt_restride",
     "dgt_get_stats", "dgt_displace", "dgt_error_string", "dgt_version", "dgt_set_timing",
     "dgt_get_phase_times", "dgt_global_triangulation_noalloc", "dgt_md_step", "dgt_md_graph_create",
-    "dgt_md_graph_launch", "dgt_md_graph_destroy", "dgt_clear_flags",
+    "dgt_md_graph_launch", "dgt_md_graph_destroy", "dgt_clear_flags", "dgt_set_kernel_shape",
+    "dgt_get_tuning", "dgt_autotune",
 ]
 STEP_AUTO = 0xFFFFFFFFFFFFFFFF
 NOALLOC_MAX_POINTS = 65536
@@ -59,6 +60,21 @@ class Stats(ctypes.Structure):
         ("reserved", ctypes.c_int),
         ("repair_calls", ctypes.c_longlong),
         ("md_step", ctypes.c_longlong),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [
+        ("cell_size", ctypes.c_double),
+        ("shape", ctypes.c_int),
+        ("trials", ctypes.c_int),
+        ("best_ms", ctypes.c_float),
+        ("default_ms", ctypes.c_float),
+        ("from_cache", ctypes.c_int),
+        ("reserved", ctypes.c_int),
     ]
 
     def as_dict(self):
@@ -125,6 +141,9 @@ def lib() -> ctypes.CDLL:
     L.dgt_md_graph_destroy.argtypes = [vp]
     L.dgt_md_graph_destroy.restype = None
     L.dgt_clear_flags.argtypes = [vp, vp]
+    L.dgt_set_kernel_shape.argtypes = [vp, ctypes.c_int]
+    L.dgt_get_tuning.argtypes = [vp, P_D, P_I, P_I, P_I]
+    L.dgt_autotune.argtypes = [vp, vp, vp, vp, ctypes.c_int, vp, ctypes.POINTER(TuneResult)]
     L.dgt_global_triangulation_noalloc.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                                    ctypes.c_double, vp, vp, ctypes.c_int, P_I, vp]
     _lib = L

@@ -16,7 +16,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
+#include <tuple>
 #include <vector>
 
 #include "dgt.h"
@@ -80,6 +83,7 @@ struct dgt_context {
     cudaEvent_t ev[DGT_NUM_PHASES][2] = {};
     bool ev_used[DGT_NUM_PHASES] = {};
     int sms = 0;
+    int shape = 0;   // kernel shape (ring capacity, block size), see dgt_set_kernel_shape
 };
 
 namespace {
@@ -294,7 +298,7 @@ cudaError_t run_slow(dgt_context *c, const RingArgs &a, cudaStream_t s)
 cudaError_t run_build(dgt_context *c, const RingArgs &a, cudaStream_t s)
 {
     c->launches += a.n_items > 0 ? 1 : 0;
-    return launch_build(a, c->precision == DGT_PRECISION_FP64 ? MODE_F64 : MODE_F32, c->sms, s);
+    return launch_build(a, c->precision == DGT_PRECISION_FP64 ? MODE_F64 : MODE_F32, c->sms, c->shape, s);
 }
 
 void to_stats(const DevStatus &d, dgt_stats *o)
@@ -744,6 +748,176 @@ void dgt_md_graph_destroy(dgt_graph *g)
     if (g->exec) cudaGraphExecDestroy(g->exec);
     if (g->graph) cudaGraphDestroy(g->graph);
     delete g;
+}
+
+int dgt_set_kernel_shape(dgt_context *c, int shape)
+{
+    if (!c || shape < 0 || shape >= KERNEL_SHAPES) return DGT_ERR_INVALID_ARGUMENT;
+    c->shape = shape;
+    return DGT_OK;
+}
+
+int dgt_get_tuning(const dgt_context *c, double *cell_size, int *shape, int *ring_capacity, int *block)
+{
+    if (!c) return DGT_ERR_INVALID_ARGUMENT;
+    if (cell_size) *cell_size = c->cell_size;
+    if (shape) *shape = c->shape;
+    if (ring_capacity) *ring_capacity = kernel_shape_cap(c->shape);
+    if (block) *block = kernel_shape_block(c->shape);
+    return DGT_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// tuned (cell size relative to the mean spacing, kernel shape) per class of input
+typedef std::tuple<int, int, int, int> TuneKey;   // log2 points, log2 sets, contrast class, precision
+std::map<TuneKey, std::pair<double, int>> g_tune_cache;
+std::mutex g_tune_mutex;
+
+__global__ void k_max_count(const int *ccount, int cells, int *out)
+{
+    int m = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cells; i += gridDim.x * blockDim.x) m = max(m, ccount[i]);
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+int ilog2(long long v)
+{
+    int r = 0;
+    while (v > 1) {
+        v >>= 1;
+        ++r;
+    }
+    return r;
+}
+
+// mean spacing of a single-set context (cell sizes are absolute there)
+double spacing_of(const dgt_context *c)
+{
+    return std::sqrt(c->boxes[0] * c->boxes[1] / std::max(c->n, 1));
+}
+
+void set_relative_cell(dgt_context *c, double rel)
+{
+    c->cell_size = c->batch ? rel : rel * spacing_of(c);
+}
+
+}  // namespace
+
+extern "C" {
+
+int dgt_autotune(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, int stride, void *stream,
+                 dgt_tune_result *out)
+{
+    if (!c || !out) return DGT_ERR_INVALID_ARGUMENT;
+    std::memset(out, 0, sizeof(*out));
+    if (c->n == 0) return DGT_OK;
+    if (!d_points || !d_tri || !d_nn || !valid_stride(stride)) return DGT_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int safety = c->safety, timing = c->timing;
+    const double cell0 = c->cell_size;
+    const int shape0 = c->shape;
+    c->safety = 1;
+    c->timing = false;
+    // density contrast of the input on the mean-spacing grid: largest cell count
+    set_relative_cell(c, 1.0);
+    int r = init_context(c);
+    if (r != DGT_OK) return r;
+    DGT_TRY(cudaMemsetAsync(c->st.p, 0, sizeof(DevStatus), s));
+    DGT_TRY(run_bin(c, d_points, s));
+    int *dmax = &c->st.as<DevStatus>()->pad;
+    DGT_TRY(cudaMemsetAsync(dmax, 0, sizeof(int), s));
+    k_max_count<<<std::min(1024, (c->total_cells + 255) / 256 + 1), 256, 0, s>>>(c->ccount.as<int>(), c->total_cells,
+                                                                                dmax);
+    int maxc = 0;
+    DGT_TRY(cudaMemcpyAsync(&maxc, dmax, sizeof(int), cudaMemcpyDeviceToHost, s));
+    DGT_TRY(cudaStreamSynchronize(s));
+    const int contrast = maxc <= 8 ? 0 : (maxc <= 32 ? 1 : 2);
+    const TuneKey key(ilog2(c->n), ilog2(c->num_sets), contrast, c->precision);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            set_relative_cell(c, it->second.first);
+            c->shape = it->second.second;
+            c->safety = safety;
+            c->timing = timing;
+            out->cell_size = c->cell_size;
+            out->shape = c->shape;
+            out->from_cache = 1;
+            return init_context(c);
+        }
+    }
+    cudaEvent_t e0, e1;
+    DGT_TRY(cudaEventCreate(&e0));
+    DGT_TRY(cudaEventCreate(&e1));
+    auto trial = [&](double rel, int shape, float *ms) -> int {
+        set_relative_cell(c, rel);
+        c->shape = shape;
+        int rr = init_context(c);
+        if (rr != DGT_OK) return rr;
+        rr = dgt_global_triangulation(c, d_points, d_tri, d_nn, stride, stream);   // warm-up
+        if (rr != DGT_OK) return rr;
+        cudaEventRecord(e0, s);
+        rr = dgt_global_triangulation(c, d_points, d_tri, d_nn, stride, stream);
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(ms, e0, e1);
+        out->trials++;
+        return rr;
+    };
+    const double rels[] = { 1.0, 0.7, 0.85, 1.2, 1.45 };
+    double best_rel = 1.0;
+    int best_shape = 0;
+    float best = 1e30f;
+    int rr = DGT_OK;
+    // any failure (including a stride too small for some ring: the caller grows the
+    // array and tunes again) ends the sweep with the original settings restored
+    for (double rel : rels) {
+        float ms = 0;
+        rr = trial(rel, 0, &ms);
+        if (rr != DGT_OK) break;
+        if (rel == 1.0) out->default_ms = ms;
+        if (ms < best) {
+            best = ms;
+            best_rel = rel;
+        }
+    }
+    for (int shape = 1; shape < KERNEL_SHAPES && rr == DGT_OK; ++shape) {
+        float ms = 0;
+        rr = trial(best_rel, shape, &ms);
+        if (rr != DGT_OK) break;
+        if (ms < best) {
+            best = ms;
+            best_shape = shape;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->safety = safety;
+    c->timing = timing;
+    if (rr != DGT_OK) {
+        c->cell_size = cell0;
+        c->shape = shape0;
+        init_context(c);
+        return rr;
+    }
+    set_relative_cell(c, best_rel);
+    c->shape = best_shape;
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        g_tune_cache[key] = std::make_pair(best_rel, best_shape);
+    }
+    out->cell_size = c->cell_size;
+    out->shape = best_shape;
+    out->best_ms = best;
+    r = init_context(c);
+    if (r != DGT_OK) return r;
+    // leave a triangulation of d_points with the chosen configuration in the outputs
+    return dgt_global_triangulation(c, d_points, d_tri, d_nn, stride, stream);
 }
 
 int dgt_clear_flags(dgt_context *c, void *stream)

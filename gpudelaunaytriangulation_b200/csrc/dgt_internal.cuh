@@ -144,7 +144,10 @@ struct TestArgs {
 cudaError_t launch_bin_st(const BinArgs &a, DevStatus *st, cudaStream_t s);
 cudaError_t launch_scan(const int *in, int n, int *bsum, int *out, cudaStream_t s);
 int scan_block_count(int n);
-cudaError_t launch_build(const RingArgs &a, int mode, int sms, cudaStream_t s);
+constexpr int KERNEL_SHAPES = 5;
+int kernel_shape_cap(int shape);
+int kernel_shape_block(int shape);
+cudaError_t launch_build(const RingArgs &a, int mode, int sms, int shape, cudaStream_t s);
 cudaError_t launch_slow(const RingArgs &a, void *scratch, int scratch_items, int capacity, cudaStream_t s);
 cudaError_t launch_test(const TestArgs &a, cudaStream_t s);
 cudaError_t launch_restride(const int *src, int old_stride, int *dst, int new_stride, const int *nn, int n,

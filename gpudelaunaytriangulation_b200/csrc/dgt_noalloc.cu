@@ -185,7 +185,7 @@ extern "C" int dgt_global_triangulation_noalloc(const double *d_points, int n, d
     r.slow_list = reinterpret_cast<int *>(base + OFF_SLOWLIST);
     r.slow_count = &d_st->slow_count;
     r.st = d_st;
-    if (launch_build(r, MODE_F32, sms, s) != cudaSuccess) return DGT_ERR_CUDA;
+    if (launch_build(r, MODE_F32, sms, 0, s) != cudaSuccess) return DGT_ERR_CUDA;
     if (launch_slow(r, base + OFF_SLOWROWS, NA_SLOW_ITEMS, 64, s) != cudaSuccess) return DGT_ERR_CUDA;
 
     // status into host stack memory (pageable: no pinned buffer is allocated)

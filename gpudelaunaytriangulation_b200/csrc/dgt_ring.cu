@@ -745,11 +745,25 @@ static cudaError_t launch_build_t(const RingArgs &a, int sms, cudaStream_t s)
     return cudaGetLastError();
 }
 
-cudaError_t launch_build(const RingArgs &a, int mode, int sms, cudaStream_t s)
+// kernel shapes the autotuner chooses from: (ring capacity on chip, threads per block)
+// index 0 is the default
+static const int kShapeCap[KERNEL_SHAPES] = { 14, 12, 16, 14, 12 };
+static const int kShapeBlock[KERNEL_SHAPES] = { 64, 64, 64, 32, 32 };
+
+int kernel_shape_cap(int shape) { return (shape >= 0 && shape < KERNEL_SHAPES) ? kShapeCap[shape] : -1; }
+int kernel_shape_block(int shape) { return (shape >= 0 && shape < KERNEL_SHAPES) ? kShapeBlock[shape] : -1; }
+
+cudaError_t launch_build(const RingArgs &a, int mode, int sms, int shape, cudaStream_t s)
 {
     if (a.n_items <= 0) return cudaSuccess;
     if (mode == MODE_F64) return launch_build_t<double, 14, 64>(a, sms, s);
-    return launch_build_t<float, 14, 64>(a, sms, s);
+    switch (shape) {
+    case 1: return launch_build_t<float, 12, 64>(a, sms, s);
+    case 2: return launch_build_t<float, 16, 64>(a, sms, s);
+    case 3: return launch_build_t<float, 14, 32>(a, sms, s);
+    case 4: return launch_build_t<float, 12, 32>(a, sms, s);
+    default: return launch_build_t<float, 14, 64>(a, sms, s);
+    }
 }
 
 cudaError_t launch_slow(const RingArgs &a, void *scratch, int scratch_items, int, cudaStream_t s)

@@ -224,6 +224,33 @@ class DelaunayGPU:
                                                _stream_ptr(stream), ctypes.byref(g)), "dgt_md_graph_create")
         return MDGraph(self._L, g, steps)
 
+    def setKernelShape(self, shape: int):
+        _nat.check(self._L.dgt_set_kernel_shape(self._h, int(shape)), "dgt_set_kernel_shape")
+
+    def tuning(self) -> dict:
+        cs, sh, cap, blk = ctypes.c_double(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _nat.check(self._L.dgt_get_tuning(self._h, ctypes.byref(cs), ctypes.byref(sh), ctypes.byref(cap),
+                                          ctypes.byref(blk)), "dgt_get_tuning")
+        return {"cell_size": cs.value, "shape": sh.value, "ring_capacity": cap.value, "block": blk.value}
+
+    def autotune(self, points: torch.Tensor, tri: torch.Tensor, nn: torch.Tensor, stream=None) -> dict:
+        """Pick cell size and kernel shape by timing builds of `points` (see dgt_autotune)."""
+        _check_points(points, self.Ncells)
+        stride = tri.numel() // max(1, self.Ncells)
+        res = _nat.TuneResult()
+        while True:
+            stride = tri.numel() // max(1, self.Ncells)
+            code = self._L.dgt_autotune(self._h, _ptr(points), _ptr(tri), _ptr(nn), stride, _stream_ptr(stream),
+                                        ctypes.byref(res))
+            if code == _nat.DGT_ERR_NEED_RESIZE and self.safetyMode:
+                tri.resize_(self.MaxSize * self.Ncells)   # grow like the triangulation calls, tune again
+                continue
+            _nat.check(code, "dgt_autotune")
+            break
+        out = res.as_dict()
+        out.update(self.tuning())
+        return out
+
     def clearFlags(self, stream=None):
         _nat.check(self._L.dgt_clear_flags(self._h, _stream_ptr(stream)), "dgt_clear_flags")
 

@@ -166,6 +166,29 @@ void dgt_md_graph_destroy(dgt_graph *graph);
 /* reset dgt_stats.sticky_flags */
 int dgt_clear_flags(dgt_context *ctx, void *stream);
 
+/* Kernel shape of the one-ring kernel: (ring entries kept on chip, threads per block) =
+ * 0: (14, 64) default, 1: (12, 64), 2: (16, 64), 3: (14, 32), 4: (12, 32).  Rings longer than
+ * the on-chip capacity continue on the exact / large-ring path, so every shape gives the same
+ * output. */
+int dgt_set_kernel_shape(dgt_context *ctx, int shape);
+int dgt_get_tuning(const dgt_context *ctx, double *cell_size, int *shape, int *ring_capacity, int *block);
+
+/* Autotuner (no reference counterpart): times global triangulations of d_points for cell
+ * edges of 0.7-1.45 mean spacings and every kernel shape, keeps the fastest on the context
+ * and caches it per (point count, set count, density contrast, precision) class for the
+ * process.  d_tri / d_neighnum receive the triangulation made with the chosen settings. */
+typedef struct dgt_tune_result {
+    double cell_size;   /* chosen cell edge (relative to the mean spacing for batched contexts) */
+    int shape;          /* chosen kernel shape */
+    int trials;
+    float best_ms;      /* build time with the chosen settings */
+    float default_ms;   /* build time with cell edge = mean spacing, shape 0 */
+    int from_cache;
+    int reserved;
+} dgt_tune_result;
+int dgt_autotune(dgt_context *ctx, const double *d_points, int *d_tri, int *d_neighnum, int stride, void *stream,
+                 dgt_tune_result *out);
+
 /* Global triangulation that allocates nothing.  No counterpart in the reference: it is
  * for callers that must not call cudaMalloc (a host application owns the GPU allocator,
  * or the memory budget is fixed before this library is loaded).  All scratch lives in one

@@ -300,3 +300,35 @@ def test_million_points_properties():
     t, k = host(tri, nn)
     assert int(k.sum()) == 6 * n
     assert_delaunay(moved, L, L, t, k, scan=False)
+
+
+def test_every_kernel_shape_same_output():
+    n = 60000
+    L = float(np.sqrt(n))
+    pts = W.uniform_points(n, L, 111)
+    ref = O.restated_global(pts, L, L, 1.0, 32)
+    for shape in range(5):
+        d = _dg()(n, 16, 1.0, (L, L))
+        d.setKernelShape(shape)
+        P = torch.from_numpy(pts).cuda()
+        tri, nn = d.globalDelaunayTriangulation(P)
+        t, k = host(tri, nn)
+        assert np.array_equal(k, ref.nn), shape
+        assert np.array_equal(O.canonical(t, k)[:, :16], O.canonical(ref.tri, ref.nn)[:, :16]), shape
+
+
+def test_autotune_result_is_correct_and_cached():
+    n = 100000
+    L = float(np.sqrt(n))
+    pts = W.uniform_points(n, L, 112)
+    d = _dg()(n, 16, 1.0, (L, L))
+    P = torch.from_numpy(pts).cuda()
+    tri = torch.zeros(16 * n, dtype=torch.int32, device="cuda")
+    nn = torch.zeros(n, dtype=torch.int32, device="cuda")
+    res = d.autotune(P, tri, nn)
+    assert res["trials"] >= 5 and 0 <= res["shape"] < 5 and res["best_ms"] <= res["default_ms"] * 1.05
+    t, k = host(tri, nn)
+    assert_delaunay(pts, L, L, t, k, scan=False)
+    d2 = _dg()(n, 16, 1.0, (L, L))
+    res2 = d2.autotune(P, tri, nn)
+    assert res2["from_cache"] == 1 and res2["shape"] == res["shape"]
