@@ -51,7 +51,6 @@ struct DevBuf {
     template <typename T> T *as() const { return reinterpret_cast<T *>(p); }
 };
 
-constexpr int SLOW_ITEMS = 2048;    // concurrent exact / large-ring items (scratch rows)
 constexpr int FIRST_ROUNDS = 3;     // repair rounds launched before the first host check
 constexpr int NEXT_ROUNDS = 2;      // rounds per later batch (each kernel exits at once on an empty list)
 constexpr int ASYNC_ROUNDS = 6;     // rounds of an unsynchronised call (convergence flagged on the device)
@@ -73,8 +72,9 @@ struct dgt_context {
     int deterministic = 1;
     std::vector<SetDesc> sets;
     int total_cells = 0;
+    int total_blocks = 0;
     DevBuf d_sets, d_set_of, ccount, cstart, cell_of, rank, sidx, slot_of, spos, bsum, mark, list0, list1,
-        slow_list, slow_scratch, st, ctl;
+        defer_list, st, ctl, bcount;
     DevStatus *h_st = nullptr;
     cudaStream_t last_stream = nullptr;
     bool stats_valid = false;
@@ -84,6 +84,7 @@ struct dgt_context {
     bool ev_used[DGT_NUM_PHASES] = {};
     int sms = 0;
     int shape = 0;   // kernel shape (ring capacity, block size), see dgt_set_kernel_shape
+    int work_budget = DEFAULT_WORK_BUDGET;   // per-point cells + candidates of the per-thread kernel
 };
 
 namespace {
@@ -149,7 +150,7 @@ double pow2_at_least(double x)
 int plan_grid(dgt_context *c)
 {
     c->sets.assign(c->num_sets, SetDesc());
-    long long cells = 0;
+    long long cells = 0, blocks = 0;
     int pbase = 0;
     for (int s = 0; s < c->num_sets; ++s) {
         double Lx = c->boxes[2 * s], Ly = c->boxes[2 * s + 1];
@@ -158,8 +159,8 @@ int plan_grid(dgt_context *c)
         double a;
         if (c->batch) a = (c->cell_size > 0 ? c->cell_size : 1.0) * spacing;
         else a = c->cell_size > 0 ? c->cell_size : spacing;
-        // keep the grid within a few cells per point (tiny cells only cost memory and scans)
-        double amin = std::sqrt(Lx * Ly / (4.0 * std::max(ns, 1) + 16.0));
+        // at most 16 cells per point (finer cells pay off only inside dense clusters)
+        double amin = std::sqrt(Lx * Ly / (16.0 * std::max(ns, 1) + 64.0));
         if (a < amin) a = amin;
         int xs = std::max(1, (int)std::floor(Lx / a));
         int ys = std::max(1, (int)std::floor(Ly / a));
@@ -178,12 +179,13 @@ int plan_grid(dgt_context *c)
         S.point_base = pbase;
         S.n = ns;
         S.V = (float)pow2_at_least(std::max(Lx, Ly));
-        S.pad = 0;
+        blocks += set_block_grid(S, (int)blocks);
         cells += (long long)xs * ys;
         pbase += ns;
         if (cells > (1LL << 30)) return DGT_ERR_INVALID_ARGUMENT;
     }
     c->total_cells = (int)cells;
+    c->total_blocks = (int)blocks;
     return DGT_OK;
 }
 
@@ -201,6 +203,7 @@ int alloc_all(dgt_context *c)
         DGT_TRY(cudaMemcpy(c->d_set_of.p, so.data(), sizeof(int) * c->n, cudaMemcpyHostToDevice));
     }
     DGT_TRY(c->ccount.ensure(sizeof(int) * C));
+    DGT_TRY(c->bcount.ensure(sizeof(int) * ((size_t)c->total_blocks + 1)));
     DGT_TRY(c->cstart.ensure(sizeof(int) * C));
     DGT_TRY(c->bsum.ensure(sizeof(int) * (scan_block_count((int)C) + 1)));
     DGT_TRY(c->cell_of.ensure(sizeof(int) * n));
@@ -210,8 +213,7 @@ int alloc_all(dgt_context *c)
     DGT_TRY(c->spos.ensure(sizeof(double2) * n));
     DGT_TRY(c->list0.ensure(sizeof(int) * n));
     DGT_TRY(c->list1.ensure(sizeof(int) * n));
-    DGT_TRY(c->slow_list.ensure(sizeof(int) * n));
-    DGT_TRY(c->slow_scratch.ensure(slow_scratch_bytes_per_item(64) * SLOW_ITEMS));
+    DGT_TRY(c->defer_list.ensure(sizeof(int) * n));
     bool fresh_mark = c->mark.bytes < sizeof(int) * (size_t)n || !c->ctl.p;
     DGT_TRY(c->mark.ensure(sizeof(int) * n));
     DGT_TRY(c->ctl.ensure(sizeof(DevCtl)));
@@ -246,6 +248,7 @@ BinArgs bin_args(dgt_context *c, const double *pts)
     a.total_cells = c->total_cells;
     a.ccount = c->ccount.as<int>();
     a.cstart = c->cstart.as<int>();
+    a.bcount = c->bcount.as<int>();
     a.cell_of = c->cell_of.as<int>();
     a.rank = c->rank.as<int>();
     a.sidx = c->sidx.as<int>();
@@ -260,6 +263,8 @@ cudaError_t run_bin(dgt_context *c, const double *pts, cudaStream_t s)
 {
     PhaseTimer t(c, DGT_PHASE_BIN, s);
     cudaError_t e = cudaMemsetAsync(c->ccount.p, 0, sizeof(int) * ((size_t)c->total_cells + 1), s);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(c->bcount.p, 0, sizeof(int) * ((size_t)c->total_blocks + 1), s);
     if (e != cudaSuccess) return e;
     c->launches += (c->n > 0 ? 2 : 0) + 3 + (c->deterministic && c->total_cells > 0 ? 1 : 0);
     return launch_bin_st(bin_args(c, pts), c->st.as<DevStatus>(), s);
@@ -276,23 +281,26 @@ RingArgs ring_args(dgt_context *c, const double *pts, int *tri, int *nn, int str
     a.sidx = c->sidx.as<int>();
     a.slot_of = c->slot_of.as<int>();
     a.cstart = c->cstart.as<int>();
+    a.bcount = c->bcount.as<int>();
     a.tri = tri;
     a.nn = nn;
     a.stride = stride;
     a.npoints = c->n;
     a.n_items = c->n;
     a.mark = c->mark.as<int>();
-    a.slow_list = c->slow_list.as<int>();
-    a.slow_count = &c->st.as<DevStatus>()->slow_count;
+    a.defer_list = c->defer_list.as<int>();
+    a.defer_count = &c->st.as<DevStatus>()->defer_count;
+    a.work_budget = c->work_budget;
     a.check = c->check;
     a.st = c->st.as<DevStatus>();
     return a;
 }
 
-cudaError_t run_slow(dgt_context *c, const RingArgs &a, cudaStream_t s)
+// the deferred points (a warp each: long rings, undecided predicates, long scans)
+cudaError_t run_deferred(dgt_context *c, const RingArgs &a, cudaStream_t s)
 {
     c->launches += 1;
-    return launch_slow(a, c->slow_scratch.p, SLOW_ITEMS, 64, s);
+    return launch_deferred(a, c->sms, s);
 }
 
 cudaError_t run_build(dgt_context *c, const RingArgs &a, cudaStream_t s)
@@ -315,6 +323,7 @@ void to_stats(const DevStatus &d, dgt_stats *o)
     o->flagged = (long long)d.flagged;
     o->repaired = (long long)d.repaired;
     o->cells = (long long)d.cells;
+    o->heavy_points = (long long)d.heavy_points;
     o->repair_rounds = d.rounds;
     o->max_ring = d.max_ring;
     o->error_flags = d.err_flags;
@@ -422,8 +431,8 @@ void dgt_destroy(dgt_context *c)
 {
     if (!c) return;
     DevBuf *bufs[] = { &c->d_sets, &c->d_set_of, &c->ccount, &c->cstart, &c->cell_of, &c->rank, &c->sidx,
-                       &c->slot_of, &c->spos, &c->bsum, &c->mark, &c->list0, &c->list1, &c->slow_list,
-                       &c->slow_scratch, &c->st, &c->ctl };
+                       &c->slot_of, &c->spos, &c->bsum, &c->mark, &c->list0, &c->list1, &c->defer_list,
+                       &c->st, &c->ctl, &c->bcount };
     for (DevBuf *b : bufs) b->release();
     if (c->h_st) cudaFreeHost(c->h_st);
     for (int p = 0; p < DGT_NUM_PHASES; ++p)
@@ -459,7 +468,7 @@ int dgt_global_triangulation(dgt_context *c, const double *d_points, int *d_tri,
     }
     {
         PhaseTimer t(c, DGT_PHASE_SLOW, s);
-        DGT_TRY(run_slow(c, a, s));
+        DGT_TRY(run_deferred(c, a, s));
     }
     c->launches += 1;
     DGT_TRY(launch_call_end(c->ctl.as<DevCtl>(), c->st.as<DevStatus>(), 0, s));
@@ -512,7 +521,7 @@ int repair_impl(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, i
         for (int b = 0; b < batch; ++b, ++round) {
             int cur = round & 1, nxt = cur ^ 1;
             DGT_TRY(cudaMemsetAsync(&dst->list_count[nxt], 0, sizeof(int), s));
-            DGT_TRY(cudaMemsetAsync(&dst->slow_count, 0, sizeof(int), s));
+            DGT_TRY(cudaMemsetAsync(&dst->defer_count, 0, sizeof(int), s));
             RingArgs a = ring_args(c, d_points, d_tri, d_nn, stride);
             a.worklist = lists[cur];
             a.worklist_count = &dst->list_count[cur];
@@ -523,7 +532,7 @@ int repair_impl(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, i
             a.next_list = lists[nxt];
             a.next_count = &dst->list_count[nxt];
             DGT_TRY(run_build(c, a, s));
-            DGT_TRY(run_slow(c, a, s));
+            DGT_TRY(run_deferred(c, a, s));
         }
         if (fixed_rounds > 0) break;
         int left = 0;
@@ -757,6 +766,13 @@ int dgt_set_kernel_shape(dgt_context *c, int shape)
     return DGT_OK;
 }
 
+int dgt_set_work_budget(dgt_context *c, int budget)
+{
+    if (!c || budget < 0) return DGT_ERR_INVALID_ARGUMENT;
+    c->work_budget = budget;
+    return DGT_OK;
+}
+
 int dgt_get_tuning(const dgt_context *c, double *cell_size, int *shape, int *ring_capacity, int *block)
 {
     if (!c) return DGT_ERR_INVALID_ARGUMENT;
@@ -828,7 +844,7 @@ int dgt_autotune(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, 
     if (r != DGT_OK) return r;
     DGT_TRY(cudaMemsetAsync(c->st.p, 0, sizeof(DevStatus), s));
     DGT_TRY(run_bin(c, d_points, s));
-    int *dmax = &c->st.as<DevStatus>()->pad;
+    int *dmax = &c->st.as<DevStatus>()->need_stride;   // scratch word: every call clears the status
     DGT_TRY(cudaMemsetAsync(dmax, 0, sizeof(int), s));
     k_max_count<<<std::min(1024, (c->total_cells + 255) / 256 + 1), 256, 0, s>>>(c->ccount.as<int>(), c->total_cells,
                                                                                 dmax);
@@ -869,7 +885,11 @@ int dgt_autotune(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, 
         out->trials++;
         return rr;
     };
-    const double rels[] = { 1.0, 0.7, 0.85, 1.2, 1.45 };
+    // uniform-ish inputs: around the mean spacing; dense clusters: much finer cells too
+    const double rels_uniform[] = { 1.0, 0.7, 0.85, 1.2, 1.45 };
+    const double rels_clustered[] = { 1.0, 0.5, 0.35, 0.25 };
+    const std::vector<double> rels = contrast < 2 ? std::vector<double>(rels_uniform, rels_uniform + 5)
+                                                  : std::vector<double>(rels_clustered, rels_clustered + 4);
     double best_rel = 1.0;
     int best_shape = 0;
     float best = 1e30f;

@@ -32,6 +32,8 @@ __global__ void __launch_bounds__(256) k_count(BinArgs a, DevStatus *st)
     int c = cell_index(S, p);
     a.cell_of[i] = c;
     a.rank[i] = atomicAdd(&a.ccount[c], 1);
+    int lc = c - S.cell_base, cy = lc / S.xsize, cx = lc - cy * S.xsize;
+    atomicAdd(&a.bcount[S.block_base + (cy >> BLOCK_SHIFT) * S.bxsize + (cx >> BLOCK_SHIFT)], 1);
 }
 
 constexpr int SCAN_THREADS = 1024;

@@ -27,36 +27,51 @@ struct SetDesc {
     int point_base;     // first point / slot of the set
     int n;              // points in the set
     float V;            // virtual corner coordinate: power of two >= max(Lx, Ly)
-    int pad;
+    int bxsize;         // occupancy blocks per row (BLOCK_CELLS x BLOCK_CELLS cells each)
+    int bysize;
+    int block_base;     // first block of the set in the block-count array
 };
+
+constexpr int BLOCK_SHIFT = 3;   // occupancy blocks of 8 x 8 cells
+constexpr int BLOCK_CELLS = 1 << BLOCK_SHIFT;
+
+// block grid of a set whose cell grid is already set; returns the number of blocks
+inline int set_block_grid(SetDesc &S, int block_base)
+{
+    S.bxsize = (S.xsize + BLOCK_CELLS - 1) / BLOCK_CELLS;
+    S.bysize = (S.ysize + BLOCK_CELLS - 1) / BLOCK_CELLS;
+    S.block_base = block_base;
+    return S.bxsize * S.bysize;
+}
 
 // device-side status / counters of one call (zeroed at the start of each call)
 struct DevStatus {
     int need_stride;            // largest ring that did not fit the caller's stride
     int max_ring;               // largest ring produced
-    int slow_count;             // items queued for the exact/large-capacity kernel
     int err_flags;              // DGT_EF_* bits
-    int list_count[2];          // repair work lists (ping-pong)
     int rounds;                 // repair rounds executed (device-side count)
+    int list_count[2];          // repair work lists (ping-pong)
+    int defer_count;            // items queued for the warp-per-point kernel
     int pad;
     unsigned long long points;          // ring constructions
     unsigned long long candidates;      // candidates examined
     unsigned long long tests;           // circle tests evaluated
     unsigned long long f32_undecided;   // undecided by the float32 filter
     unsigned long long f64_undecided;   // undecided by the float64 recheck
-    unsigned long long exact_points;    // points run through exact arithmetic
+    unsigned long long exact_points;    // deferred points (warp-per-point kernel: float64 + exact)
     unsigned long long capacity_points; // points whose ring outgrew on-chip capacity
     unsigned long long mismatches;      // check mode: filter decisions contradicted by float64
     unsigned long long insertions;      // ring insertions
     unsigned long long flagged;         // points queued by the test kernel
     unsigned long long repaired;        // points rebuilt by repair rounds
     unsigned long long cells;           // grid cells scanned
+    unsigned long long heavy_points;    // deferred because they outgrew the per-thread work budget
 };
 
 enum : int {
     EF_UNBOUNDED = 1,      // a ring still held a virtual corner after the whole box was scanned
     EF_NONCONTIG = 2,      // a conflict set was not one contiguous arc (degenerate input)
-    EF_SLOW_OVERFLOW = 4,  // a ring outgrew even the large-capacity path
+    EF_SLOW_OVERFLOW = 4,  // a ring outgrew even the 64 entries of the deferred path
     EF_EXACT_UNRESOLVED = 8,
     EF_BAD_INPUT = 16,     // coordinates not finite
     // warning, not an error: a certified circle reached past half the box, where minimum-
@@ -84,6 +99,7 @@ struct BinArgs {
     int total_cells;
     int *ccount;     // total_cells + 1
     int *cstart;     // total_cells + 1
+    int *bcount;     // points per occupancy block (zeroed by the caller)
     int *cell_of;    // n
     int *rank;       // n
     int *sidx, *slot_of;
@@ -100,6 +116,7 @@ struct RingArgs {
     const int *sidx;
     const int *slot_of;
     const int *cstart;
+    const int *bcount;  // points per occupancy block: empty blocks are skipped by the scan
     int *tri;
     int *nn;
     int stride;
@@ -116,9 +133,12 @@ struct RingArgs {
     int round;
     int *next_list;
     int *next_count;
-    // deferred items for the exact / large-capacity kernel
-    int *slow_list;
-    int *slow_count;
+    // points deferred to the warp-per-point kernel (float64 + exact, 64-entry ring): rings
+    // longer than the per-thread capacity, predicates float32 and float64 cannot decide, and
+    // scans longer than work_budget (cells + candidates)
+    int *defer_list;
+    int *defer_count;
+    int work_budget;
     int check;         // 1: count float32 decisions contradicted by float64
     DevStatus *st;
 };
@@ -148,7 +168,8 @@ constexpr int KERNEL_SHAPES = 5;
 int kernel_shape_cap(int shape);
 int kernel_shape_block(int shape);
 cudaError_t launch_build(const RingArgs &a, int mode, int sms, int shape, cudaStream_t s);
-cudaError_t launch_slow(const RingArgs &a, void *scratch, int scratch_items, int capacity, cudaStream_t s);
+cudaError_t launch_deferred(const RingArgs &a, int sms, cudaStream_t s);
+constexpr int DEFAULT_WORK_BUDGET = 4096;
 cudaError_t launch_test(const TestArgs &a, cudaStream_t s);
 cudaError_t launch_restride(const int *src, int old_stride, int *dst, int new_stride, const int *nn, int n,
                             cudaStream_t s);
@@ -159,8 +180,5 @@ cudaError_t launch_displace(double2 *pos, int n, const SetDesc *sets, const int 
 // end of a test-and-repair call: fold flags into the sticky word, check convergence,
 // advance the epoch by rounds + 1
 cudaError_t launch_call_end(DevCtl *ctl, DevStatus *st, int rounds, cudaStream_t s);
-size_t slow_scratch_bytes_per_item(int capacity);
-// bytes of one row of the exact / large-ring path (64 entries of double4 + double2 + int)
-constexpr size_t SLOW_ROW_BYTES = 64 * (sizeof(double4) + sizeof(double2) + sizeof(int));
 
 }  // namespace dgt

@@ -34,7 +34,6 @@ namespace {
 
 constexpr int NA_MAX_POINTS = DGT_NOALLOC_MAX_POINTS;
 constexpr int NA_MAX_CELLS = DGT_NOALLOC_MAX_CELLS;
-constexpr int NA_SLOW_ITEMS = 64;
 constexpr size_t NA_ALIGN = 256;
 
 constexpr size_t up(size_t x) { return (x + NA_ALIGN - 1) / NA_ALIGN * NA_ALIGN; }
@@ -49,10 +48,12 @@ constexpr size_t OFF_CELLOF = OFF_BSUM + up(sizeof(int) * ((NA_MAX_CELLS + 1) / 
 constexpr size_t OFF_RANK = OFF_CELLOF + up(sizeof(int) * NA_MAX_POINTS);
 constexpr size_t OFF_SIDX = OFF_RANK + up(sizeof(int) * NA_MAX_POINTS);
 constexpr size_t OFF_SLOTOF = OFF_SIDX + up(sizeof(int) * NA_MAX_POINTS);
-constexpr size_t OFF_SLOWLIST = OFF_SLOTOF + up(sizeof(int) * NA_MAX_POINTS);
-constexpr size_t OFF_SPOS = OFF_SLOWLIST + up(sizeof(int) * NA_MAX_POINTS);
-constexpr size_t OFF_SLOWROWS = OFF_SPOS + up(sizeof(double2) * NA_MAX_POINTS);
-constexpr size_t NA_BYTES = OFF_SLOWROWS + up(SLOW_ROW_BYTES * NA_SLOW_ITEMS);
+constexpr size_t OFF_DEFERLIST = OFF_SLOTOF + up(sizeof(int) * NA_MAX_POINTS);
+constexpr size_t OFF_SPOS = OFF_DEFERLIST + up(sizeof(int) * NA_MAX_POINTS);
+// occupancy blocks: bx*by <= cells/64 + (xsize+ysize)/8 + 1 <= cells/4 + 16
+constexpr size_t NA_MAX_BLOCKS = NA_MAX_CELLS / 4 + 16;
+constexpr size_t OFF_BCOUNT = OFF_SPOS + up(sizeof(double2) * NA_MAX_POINTS);
+constexpr size_t NA_BYTES = OFF_BCOUNT + up(sizeof(int) * NA_MAX_BLOCKS);
 
 }  // namespace
 
@@ -90,14 +91,16 @@ double pow2_at_least(double x)
 }  // namespace
 
 // writes the set descriptor and clears what must start at zero (cell counts, status)
-__global__ void k_noalloc_setup(SetDesc S, SetDesc *sets, DevStatus *st, int *ccount, int ncount)
+__global__ void k_noalloc_setup(SetDesc S, SetDesc *sets, DevStatus *st, int *ccount, int ncount, int *bcount,
+                                int nblocks)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {
         *sets = S;
         *st = DevStatus();
     }
-    for (; i < ncount; i += gridDim.x * blockDim.x) ccount[i] = 0;
+    for (int k = i; k < ncount; k += gridDim.x * blockDim.x) ccount[k] = 0;
+    for (int k = i; k < nblocks; k += gridDim.x * blockDim.x) bcount[k] = 0;
 }
 
 extern "C" int dgt_global_triangulation_noalloc(const double *d_points, int n, double Lx, double Ly,
@@ -113,7 +116,7 @@ extern "C" int dgt_global_triangulation_noalloc(const double *d_points, int n, d
     // cell grid (same rule as a context: requested edge, no finer than ~4 cells per point)
     double spacing = std::sqrt(Lx * Ly / n);
     double a = cell_size > 0 ? cell_size : spacing;
-    double amin = std::sqrt(Lx * Ly / (4.0 * n + 16.0));
+    double amin = std::sqrt(Lx * Ly / (4.0 * n + 16.0));   // at most ~4 cells per point here
     if (a < amin) a = amin;
     int xs = std::max(1, (int)std::floor(Lx / a)), ys = std::max(1, (int)std::floor(Ly / a));
     if ((long long)xs * ys > NA_MAX_CELLS) return DGT_ERR_INVALID_ARGUMENT;
@@ -132,8 +135,9 @@ extern "C" int dgt_global_triangulation_noalloc(const double *d_points, int n, d
     S.point_base = 0;
     S.n = n;
     S.V = (float)pow2_at_least(std::max(Lx, Ly));
-    S.pad = 0;
+    const int blocks = set_block_grid(S, 0);
     const int cells = xs * ys;
+    if ((size_t)blocks > NA_MAX_BLOCKS) return DGT_ERR_INVALID_ARGUMENT;
 
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return DGT_ERR_CUDA;
@@ -148,7 +152,9 @@ extern "C" int dgt_global_triangulation_noalloc(const double *d_points, int n, d
     DevStatus *d_st = reinterpret_cast<DevStatus *>(base + OFF_STATUS);
     k_noalloc_setup<<<std::min((cells + 1 + 255) / 256, 1024), 256, 0, s>>>(S, d_sets, d_st,
                                                                           reinterpret_cast<int *>(base + OFF_CCOUNT),
-                                                                          cells + 1);
+                                                                          cells + 1,
+                                                                          reinterpret_cast<int *>(base + OFF_BCOUNT),
+                                                                          blocks);
     if (cudaGetLastError() != cudaSuccess) return DGT_ERR_CUDA;
 
     BinArgs b;
@@ -165,6 +171,7 @@ extern "C" int dgt_global_triangulation_noalloc(const double *d_points, int n, d
     b.slot_of = reinterpret_cast<int *>(base + OFF_SLOTOF);
     b.spos = reinterpret_cast<double2 *>(base + OFF_SPOS);
     b.block_sums = reinterpret_cast<int *>(base + OFF_BSUM);
+    b.bcount = reinterpret_cast<int *>(base + OFF_BCOUNT);
     b.deterministic = 1;
     if (launch_bin_st(b, d_st, s) != cudaSuccess) return DGT_ERR_CUDA;
 
@@ -177,16 +184,18 @@ extern "C" int dgt_global_triangulation_noalloc(const double *d_points, int n, d
     r.sidx = b.sidx;
     r.slot_of = b.slot_of;
     r.cstart = b.cstart;
+    r.bcount = b.bcount;
     r.tri = d_tri;
     r.nn = d_neighnum;
     r.stride = stride;
     r.npoints = n;
     r.n_items = n;
-    r.slow_list = reinterpret_cast<int *>(base + OFF_SLOWLIST);
-    r.slow_count = &d_st->slow_count;
+    r.defer_list = reinterpret_cast<int *>(base + OFF_DEFERLIST);
+    r.defer_count = &d_st->defer_count;
+    r.work_budget = DEFAULT_WORK_BUDGET;
     r.st = d_st;
     if (launch_build(r, MODE_F32, sms, 0, s) != cudaSuccess) return DGT_ERR_CUDA;
-    if (launch_slow(r, base + OFF_SLOWROWS, NA_SLOW_ITEMS, 64, s) != cudaSuccess) return DGT_ERR_CUDA;
+    if (launch_deferred(r, sms, s) != cudaSuccess) return DGT_ERR_CUDA;
 
     // status into host stack memory (pageable: no pinned buffer is allocated)
     DevStatus h;

@@ -17,17 +17,42 @@
 //   4. write the ring rotated to start at its smallest index (a canonical start; the
 //      reference's start depends on insertion order) into row p of the caller's array.
 // The ring lives in shared memory (per-thread columns, conflict-free).  Points whose ring
-// outgrows that capacity, or that meet a predicate neither float32 nor float64 can decide,
-// are re-run by a large-capacity kernel with exact arithmetic (slow path).
+// outgrows that capacity, that meet a predicate neither float32 nor float64 can decide, or
+// whose scan outgrows a work budget are rebuilt by a warp each (float64 + exact arithmetic,
+// 64-entry ring; k_build_warp).
 #include "dgt_internal.cuh"
 #include "dgt_predicates.cuh"
 
 namespace dgt {
 
-enum { R_OK = 0, R_CAPACITY = 1, R_EXACT = 2, R_UNBOUNDED = 3, R_NONCONTIG = 4 };
+enum { R_OK = 0, R_CAPACITY = 1, R_EXACT = 2, R_UNBOUNDED = 3, R_NONCONTIG = 4, R_HEAVY = 5 };
 
+// statistics of one thread
 struct Ctr {
     unsigned cand, tests, u32, u64, ins, mism, cells;
+    __device__ __forceinline__ void add_u32() { u32++; }
+    __device__ __forceinline__ void add_u64() { u64++; }
+    __device__ __forceinline__ void add_ins() { ins++; }
+    __device__ __forceinline__ void add_mism(unsigned v) { mism += v; }
+    __device__ __forceinline__ void add_cells() { cells++; }
+    __device__ __forceinline__ Ctr total() const { return *this; }
+};
+// the same, with the rarely bumped counters in shared memory (one column per thread): the
+// per-thread kernel's registers are what limits its occupancy
+template <int BLOCK>
+struct SmemCtr {
+    unsigned cand, tests;
+    unsigned (*rare)[BLOCK];   // rows: u32, u64, ins, mism, cells
+    __device__ __forceinline__ void add_u32() { rare[0][threadIdx.x]++; }
+    __device__ __forceinline__ void add_u64() { rare[1][threadIdx.x]++; }
+    __device__ __forceinline__ void add_ins() { rare[2][threadIdx.x]++; }
+    __device__ __forceinline__ void add_mism(unsigned v) { rare[3][threadIdx.x] += v; }
+    __device__ __forceinline__ void add_cells() { rare[4][threadIdx.x]++; }
+    __device__ __forceinline__ Ctr total() const
+    {
+        const int t = threadIdx.x;
+        return Ctr{ cand, tests, rare[0][t], rare[1][t], rare[2][t], rare[3][t], rare[4][t] };
+    }
 };
 
 // ---------------------------------------------------------------- ring storage policies
@@ -38,8 +63,10 @@ struct SmemRing {
     E4 (*e)[BLOCK];
     V2 (*v)[BLOCK];
     int (*id)[BLOCK];
+    int *wk;   // per-thread scan work of the current point (per-thread kernel only)
     int t;
     static constexpr int cap = CAP;
+    __device__ __forceinline__ int &work() { return wk[t]; }
     __device__ __forceinline__ E4 edge(int k) const { return e[k][t]; }
     __device__ __forceinline__ V2 vert(int k) const { return v[k][t]; }
     __device__ __forceinline__ int idx(int k) const { return id[k][t]; }
@@ -50,27 +77,6 @@ struct SmemRing {
         e[dst][t] = e[src][t];
         v[dst][t] = v[src][t];
         id[dst][t] = id[src][t];
-    }
-};
-
-template <typename T, int CAP>
-struct GlobalRing {
-    typedef typename Prec<T>::T4 E4;
-    typedef typename Prec<T>::T2 V2;
-    E4 *e;
-    V2 *v;
-    int *id;
-    static constexpr int cap = CAP;
-    __device__ __forceinline__ E4 edge(int k) const { return e[k]; }
-    __device__ __forceinline__ V2 vert(int k) const { return v[k]; }
-    __device__ __forceinline__ int idx(int k) const { return id[k]; }
-    __device__ __forceinline__ void set_edge(int k, E4 x) { e[k] = x; }
-    __device__ __forceinline__ void set_vert(int k, V2 x, int i) { v[k] = x; id[k] = i; }
-    __device__ __forceinline__ void move(int dst, int src)
-    {
-        e[dst] = e[src];
-        v[dst] = v[src];
-        id[dst] = id[src];
     }
 };
 
@@ -138,7 +144,7 @@ __device__ __noinline__ double4 circle64(const double2 *pos, double2 p, double L
 }
 
 // ------------------------------------------------------------------- the construction
-template <typename T, bool EXACT, class Ring>
+template <typename T, bool EXACT, class Ring, class C = Ctr>
 struct Builder {
     typedef Prec<T> PR;
     typedef typename PR::T4 E4;
@@ -148,7 +154,7 @@ struct Builder {
     const RingArgs &A;
     const SetDesc &S;
     Ring &R;
-    Ctr &ctr;
+    C &ctr;
     double2 p;
     int slot;
     int m;
@@ -156,7 +162,7 @@ struct Builder {
     int ocx, ocy;
     bool minimage = false;   // the certified circles reach past half the box
 
-    __device__ Builder(const RingArgs &a, const SetDesc &s, Ring &r, Ctr &c, double2 pp, int sl)
+    __device__ Builder(const RingArgs &a, const SetDesc &s, Ring &r, C &c, double2 pp, int sl)
         : A(a), S(s), R(r), ctr(c), p(pp), slot(sl), m(0), r2max((T)0), ocx(0), ocy(0) {}
 
     __device__ void refresh_r2max()
@@ -169,7 +175,8 @@ struct Builder {
         r2max = (T)4 * mx * mx * ((T)1 + (T)64 * PR::u());
     }
 
-    __device__ void init()
+    // the square of virtual corners (ring storage only)
+    __device__ void init_ring()
     {
         T V = (T)S.V;
         for (int c = 0; c < 4; ++c) R.set_vert(c, corner<T>(c, V), -1 - c);
@@ -177,11 +184,21 @@ struct Builder {
             V2 a = corner<T>(c, V), b = corner<T>((c + 1) & 3, V);
             R.set_edge(c, make_circ<T>(a.x, a.y, b.x, b.y));
         }
+    }
+    // per-thread state of a fresh ring (reads the ring storage)
+    __device__ void init_local()
+    {
+        if (!EXACT) R.work() = 0;
         m = 4;
         refresh_r2max();
         int cx = (int)floor(p.x * S.icw), cy = (int)floor(p.y * S.ich);
         ocx = min(max(cx, 0), S.xsize - 1);
         ocy = min(max(cy, 0), S.ysize - 1);
+    }
+    __device__ void init()
+    {
+        init_ring();
+        init_local();
     }
 
     // float64 (then, on the exact path, exact) decision for edge k against candidate d:
@@ -190,7 +207,7 @@ struct Builder {
     {
         int ia = R.idx(k), ib = R.idx(k + 1 == m ? 0 : k + 1);
         int r = recheck64<EXACT>(A.pos, p, S.Lx, S.hLx, S.Ly, S.hLy, S.V, ia, ib, d64.x, d64.y);
-        if (r == 2 || r == -2 || r == 0) ctr.u64++;
+        if (r == 2 || r == -2 || r == 0) ctr.add_u64();
         return r > 0 ? 1 : (r < 0 ? -1 : 0);
     }
 
@@ -225,26 +242,27 @@ struct Builder {
         R.set_vert(ns + 1, d, id);
         R.set_edge(ns + 1, cb);
         m = mnew;
-        ctr.ins++;
+        ctr.add_ins();
         refresh_r2max();
         return R_OK;
     }
 
-    // one candidate (cell-order slot sl): filter every ring edge, settle undecided ones,
-    // insert on conflict
-    __device__ __forceinline__ int candidate(int sl)
+    // one candidate (cell-order slot sl) against every ring edge: `mask` gets the edges whose
+    // circle holds it strictly inside (undecided filters settled by recheck); d its offset
+    __device__ __forceinline__ int classify(int sl, V2 &d, Mask &mask)
     {
+        mask = 0;
         if (sl == slot) return R_OK;
         double2 q = __ldg(&A.spos[sl]);
         double2 d64 = make_double2(wrap_off(q.x, p.x, S.Lx, S.hLx), wrap_off(q.y, p.y, S.Ly, S.hLy));
         if (d64.x == 0.0 && d64.y == 0.0) return R_OK;   // coincident point
         ctr.cand++;
-        V2 d = PR::mk2(PR::from64(d64.x), PR::from64(d64.y));
+        d = PR::mk2(PR::from64(d64.x), PR::from64(d64.y));
         T nd = d.x * d.x + d.y * d.y;
         if (nd > r2max) return R_OK;
         T ad = sqrt_up(nd);   // only scales the bound: an upper value is safe
         T kb = (T)8 * PR::u() * nd + PR::tiny();
-        Mask mask = 0, open = 0;
+        Mask open = 0;
         for (int k = 0; k < m; ++k) {
             E4 e = R.edge(k);
             T sv = fma(d.x, e.x, fma(d.y, e.y, -nd));
@@ -256,7 +274,7 @@ struct Builder {
         if (open) {
             for (int k = 0; k < m; ++k) {
                 if (!((open >> k) & 1)) continue;
-                ctr.u32++;
+                ctr.add_u32();
                 int r = recheck(k, d64);
                 if (r == 0) return R_EXACT;
                 if (r > 0) mask |= (Mask)1 << k;
@@ -266,11 +284,20 @@ struct Builder {
             for (int k = 0; k < m; ++k) {
                 if ((open >> k) & 1) continue;
                 int ia = R.idx(k), ib = R.idx(k + 1 == m ? 0 : k + 1);
-                ctr.mism += check64(A.pos, p, S.Lx, S.hLx, S.Ly, S.hLy, S.V, ia, ib, d64.x, d64.y,
-                                    (int)((mask >> k) & 1));
+                ctr.add_mism(check64(A.pos, p, S.Lx, S.hLx, S.Ly, S.hLy, S.V, ia, ib, d64.x, d64.y,
+                                    (int)((mask >> k) & 1)));
             }
         }
-        if (!mask) return R_OK;
+        return R_OK;
+    }
+
+    // one candidate: classify, insert on conflict
+    __device__ __forceinline__ int candidate(int sl)
+    {
+        V2 d;
+        Mask mask;
+        int r = classify(sl, d, mask);
+        if (r != R_OK || !mask) return r;
         return insert(d, __ldg(&A.sidx[sl]), mask);
     }
 
@@ -322,9 +349,10 @@ struct Builder {
                     growth_cell(g, ci++, rx, ry);
                     int cx = wrapi(ocx + rx, S.xsize), cy = wrapi(ocy + ry, S.ysize);
                     int c = S.cell_base + cy * S.xsize + cx;
-                    ctr.cells++;
+                    ctr.add_cells();
                     sl = __ldg(&A.cstart[c]);
                     se = __ldg(&A.cstart[c + 1]);
+                    if (!EXACT) R.work() += 1 + se - sl;   // checked against the budget per phase
                 }
                 have = sl < se;
             }
@@ -380,6 +408,32 @@ struct Builder {
         return true;
     }
 
+    // Whether the cell (rx, ry) (relative to the own cell) may hold a point strictly inside
+    // some edge circle: its rectangle, widened by a margin far above the rounding of cell
+    // indices and offsets, meets a disc (c~, rc) that contains the exact circle.  Cells
+    // across the minimum-image seam are always reached.  A cell not reached stays so: the
+    // union of the circles through p of a star-shaped ring only shrinks under insertion (a
+    // disc through p centred in the convex Voronoi cell lies in the union of the discs centred
+    // at the cell's vertices, because d - c, |d - c|^2 - |p - c|^2 is affine in c).
+    __device__ bool cell_reached(int rx, int ry, double fx, double fy)
+    {
+        const double mg = 1e-9;
+        double a0 = (double)rx - fx, a1 = a0 + 1.0, b0 = (double)ry - fy, b1 = b0 + 1.0;
+        a0 = (a0 - mg * (1.0 + fabs(a0))) * S.cw;
+        a1 = (a1 + mg * (1.0 + fabs(a1))) * S.cw;
+        b0 = (b0 - mg * (1.0 + fabs(b0))) * S.ch;
+        b1 = (b1 + mg * (1.0 + fabs(b1))) * S.ch;
+        if (a0 < -S.hLx || a1 > S.hLx || b0 < -S.hLy || b1 > S.hLy) return true;
+        for (int k = 0; k < m; ++k) {
+            E4 e = R.edge(k);
+            if (!(e.w < PR::inf())) return true;
+            double cx = 0.5 * (double)e.x, cy = 0.5 * (double)e.y, rc = (double)e.w * (1.0 + mg);
+            double dx = fmax(fmax(a0 - cx, cx - a1), 0.0), dy = fmax(fmax(b0 - cy, cy - b1), 0.0);
+            if (dx * dx + dy * dy <= rc * rc) return true;
+        }
+        return false;
+    }
+
     // Called by every lane of the warp (warp votes inside); `active` false for lanes
     // without a point.  Returns R_OK / error for active lanes.
     __device__ int run(bool active)
@@ -421,6 +475,8 @@ struct Builder {
             int r = scan(growth(x0, x1, y0, y1, gx0, gx1, gy0, gy1, phase == 0), live);
             if (live) {
                 if (r != R_OK) status = r;
+                // over the work budget: the warp-per-point kernel takes the point over
+                if (!EXACT && status == R_OK && R.work() > A.work_budget) status = R_HEAVY;
                 x0 = gx0; x1 = gx1; y0 = gy0; y1 = gy1;
             }
             if (__all_sync(0xffffffffu, done || status != R_OK)) break;
@@ -529,8 +585,11 @@ __global__ void __launch_bounds__(BLOCK) k_build(RingArgs A)
     __shared__ E4 se[CAP][BLOCK];
     __shared__ V2 sv[CAP][BLOCK];
     __shared__ int si[CAP][BLOCK];
-    SmemRing<T, CAP, BLOCK> ring{ se, sv, si, (int)threadIdx.x };
-    Ctr ctr = { 0, 0, 0, 0, 0, 0, 0 };
+    __shared__ int swork[BLOCK];
+    __shared__ unsigned srare[5][BLOCK];
+    SmemRing<T, CAP, BLOCK> ring{ se, sv, si, swork, (int)threadIdx.x };
+    for (int k = 0; k < 5; ++k) srare[k][threadIdx.x] = 0;
+    SmemCtr<BLOCK> ctr{ 0, 0, srare };
     unsigned pts = 0;
     int maxr = 0;
     const int n = item_count(A);
@@ -554,72 +613,217 @@ __global__ void __launch_bounds__(BLOCK) k_build(RingArgs A)
         }
         const SetDesc S = A.sets[(act && A.set_of) ? __ldg(&A.set_of[slot]) : 0];
         double2 p = act ? __ldg(&A.spos[slot]) : make_double2(0.0, 0.0);
-        Builder<T, false, SmemRing<T, CAP, BLOCK>> b(A, S, ring, ctr, p, slot);
+        Builder<T, false, SmemRing<T, CAP, BLOCK>, SmemCtr<BLOCK>> b(A, S, ring, ctr, p, slot);
         int r = b.run(act);
         if (act) {
             pts++;
             if (r == R_OK) {
                 finish(A, pid, ring, b.m, maxr);
-            } else if (r == R_CAPACITY || r == R_EXACT) {
-                A.slow_list[atomicAdd(A.slow_count, 1)] = pid;
+            } else if (r == R_CAPACITY || r == R_EXACT || r == R_HEAVY) {
+                // over-budget points go in complemented (counted by the warp kernel)
+                A.defer_list[atomicAdd(A.defer_count, 1)] = r == R_HEAVY ? ~pid : pid;
             } else {
                 atomicOr(&A.st->err_flags, r == R_UNBOUNDED ? EF_UNBOUNDED : EF_NONCONTIG);
                 A.nn[pid] = 0;
             }
         }
     }
-    flush_counters(A, ctr, pts, maxr);
+    flush_counters(A, ctr.total(), pts, maxr);
 }
 
-// slow kernel: double + exact arithmetic, ring of 64 entries in a global scratch row per
-// thread; grid-stride over the device-side slow list
-constexpr int SLOW_CAP = 64;
+// ------------------------------------------------------------ deferred points: a warp per point
+// Points the per-thread kernel hands on -- rings longer than its capacity, predicates neither
+// float32 nor float64 decides, and scans longer than the work budget (typically on the rim of
+// dense clusters, where the circles reach over large, partly empty and partly dense regions)
+// -- are rebuilt by a whole warp.  The 32 lanes share one ring in shared memory (float64
+// filter, exact residue, 64 entries), take 32 new cells at a time (dropping empty occupancy
+// blocks and cells that no current circle reaches) and 32 candidates at a time.  One lane inserts; lanes whose
+// candidates conflicted test them again against the new ring (a candidate outside every
+// circle stays outside, see cell_reached).  The scanned rectangle grows one cell per side
+// while the ring keeps changing, by half its extent while virtual corners are left, and
+// straight to the circles' cells once a layer changed nothing.
+constexpr int WARP_KERNEL_CAP = 64;
+constexpr int WARP_KERNEL_WARPS = 4;   // warps (points) per block
 
-template <typename T>
-struct SlowRow {
-    typename Prec<T>::T4 e[SLOW_CAP];
-    typename Prec<T>::T2 v[SLOW_CAP];
-    int id[SLOW_CAP];
-};
-
-__global__ void __launch_bounds__(64) k_build_slow(RingArgs A, SlowRow<double> *scratch, int scratch_items)
+// New extent [g0,g1] of one axis: towards the needed [lo,hi] by at most `step` per side,
+// never wider than the grid (a full-width extent covers every cell of the axis once)
+__device__ __forceinline__ void grow_axis(int a0, int a1, int lo, int hi, int step, int size, int &g0, int &g1)
 {
-    int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    g0 = a0;
+    g1 = a1;
+    int room = size - (a1 - a0 + 1);
+    if (room <= 0) return;
+    int want_lo = lo < a0 ? min(a0 - lo, step) : 0;
+    int want_hi = hi > a1 ? min(hi - a1, step) : 0;
+    if (want_lo + want_hi > room) {
+        int l = min(want_lo, room - min(want_hi, room / 2));
+        want_hi = min(want_hi, room - l);
+        want_lo = l;
+    }
+    g0 = a0 - want_lo;
+    g1 = a1 + want_hi;
+}
+
+template <class B>
+__device__ int coop_run(B &b, const int lane)
+{
+    typedef typename B::Mask Mask;
+    typedef typename B::V2 V2;
+    const RingArgs &A = b.A;
+    const SetDesc &S = b.S;
+    if (lane == 0) b.init_ring();
+    __syncwarp();
+    b.init_local();
+    const double fx = b.p.x * S.icw - (double)b.ocx, fy = b.p.y * S.ich - (double)b.ocy;
+    int x0 = 0, x1 = 0, y0 = 0, y1 = 0;
+    bool changed = true;
+    int status = R_OK;
+    const int max_phase = S.xsize + S.ysize + 8;
+    for (int phase = 0; status == R_OK && phase < max_phase; ++phase) {
+        int nx0 = x0, nx1 = x1, ny0 = y0, ny1 = y1;
+        if (phase == 1) {
+            nx0 = S.xsize >= 3 ? -1 : 0;
+            nx1 = S.xsize >= 2 ? 1 : 0;
+            ny0 = S.ysize >= 3 ? -1 : 0;
+            ny1 = S.ysize >= 2 ? 1 : 0;
+        } else if (phase > 1) {
+            int lx, hx, ly, hy;
+            if (!b.need_rect(fx, fy, lx, hx, ly, hy)) {
+                lx = ly = -(1 << 28);
+                hx = hy = 1 << 28;
+            }
+            bool real = true;
+            for (int k = 0; k < b.m; ++k) real &= b.R.idx(k) >= 0;
+            const int sx = changed ? 1 : (real ? (1 << 28) : max(1, (x1 - x0 + 1) >> 1));
+            const int sy = changed ? 1 : (real ? (1 << 28) : max(1, (y1 - y0 + 1) >> 1));
+            grow_axis(x0, x1, lx, hx, sx, S.xsize, nx0, nx1);
+            grow_axis(y0, y1, ly, hy, sy, S.ysize, ny0, ny1);
+            if (nx0 == x0 && nx1 == x1 && ny0 == y0 && ny1 == y1) break;
+        }
+        changed = false;
+        // new cells: columns left and right of the old rectangle (nearest first, over its
+        // rows), then rows below and above (over the new columns)
+        const int h = y1 - y0 + 1, w = nx1 - nx0 + 1;
+        const int nl = (x0 - nx0) * h, nr = (nx1 - x1) * h, nb = (y0 - ny0) * w, nt = (ny1 - y1) * w;
+        const int ncell = phase == 0 ? 1 : nl + nr + nb + nt;
+        for (int cb = 0; cb < ncell && status == R_OK; cb += 32) {
+            int ci = cb + lane, start = 0, cnt = 0;
+            if (ci < ncell) {
+                int rx = 0, ry = 0;
+                if (phase > 0) {
+                    if (ci < nl) {
+                        rx = x0 - 1 - ci / h;
+                        ry = y0 + ci % h;
+                    } else if ((ci -= nl) < nr) {
+                        rx = x1 + 1 + ci / h;
+                        ry = y0 + ci % h;
+                    } else if ((ci -= nr) < nb) {
+                        ry = y0 - 1 - ci / w;
+                        rx = nx0 + ci % w;
+                    } else {
+                        ci -= nb;
+                        ry = y1 + 1 + ci / w;
+                        rx = nx0 + ci % w;
+                    }
+                }
+                const int cx = wrapi(b.ocx + rx, S.xsize), cy = wrapi(b.ocy + ry, S.ysize);
+                const int blk = S.block_base + (cy >> BLOCK_SHIFT) * S.bxsize + (cx >> BLOCK_SHIFT);
+                if (__ldg(&A.bcount[blk]) != 0 && (phase < 2 || b.cell_reached(rx, ry, fx, fy))) {
+                    const int c = S.cell_base + cy * S.xsize + cx;
+                    start = __ldg(&A.cstart[c]);
+                    cnt = __ldg(&A.cstart[c + 1]) - start;
+                    b.ctr.add_cells();
+                }
+            }
+            int incl = cnt;
+            for (int o = 1; o < 32; o <<= 1) {
+                int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const int total = __shfl_sync(0xffffffffu, incl, 31), excl = incl - cnt;
+            for (int j0 = 0; j0 < total && status == R_OK; j0 += 32) {
+                const int j = j0 + lane;
+                int o = 0;   // the last lane whose cell range starts at or before j
+                for (int step = 16; step > 0; step >>= 1) {
+                    int e = __shfl_sync(0xffffffffu, excl, o + step);
+                    if (e <= j) o += step;
+                }
+                const int sl = __shfl_sync(0xffffffffu, start, o) + j - __shfl_sync(0xffffffffu, excl, o);
+                const bool have = j < total;
+                V2 d = make_double2(0.0, 0.0);
+                Mask mask = 0;
+                if (have) b.classify(sl, d, mask);
+                unsigned want = __ballot_sync(0xffffffffu, have && mask != 0);
+                while (want) {
+                    const int leader = __ffs(want) - 1;
+                    int ir = R_OK;
+                    if (lane == leader) ir = b.insert(d, __ldg(&A.sidx[sl]), mask);
+                    ir = __shfl_sync(0xffffffffu, ir, leader);
+                    b.m = __shfl_sync(0xffffffffu, b.m, leader);
+                    b.r2max = __shfl_sync(0xffffffffu, b.r2max, leader);
+                    __syncwarp();
+                    if (ir != R_OK) {
+                        status = ir;
+                        break;
+                    }
+                    changed = true;
+                    const bool again = ((want >> lane) & 1u) && lane != leader;
+                    mask = 0;
+                    if (again) b.classify(sl, d, mask);
+                    want = __ballot_sync(0xffffffffu, again && mask != 0);
+                }
+            }
+        }
+        x0 = nx0;
+        x1 = nx1;
+        y0 = ny0;
+        y1 = ny1;
+    }
+    if (status != R_OK) return status;
+    for (int k = 0; k < b.m; ++k)
+        if (b.R.idx(k) < 0) return R_UNBOUNDED;
+    if (b.minimage && lane == 0) atomicOr(&A.st->err_flags, EF_MINIMAGE);
+    return R_OK;
+}
+
+__global__ void __launch_bounds__(WARP_KERNEL_WARPS * 32, 4) k_build_warp(RingArgs A)
+{
+    __shared__ double4 se[WARP_KERNEL_CAP][WARP_KERNEL_WARPS];
+    __shared__ double2 sv[WARP_KERNEL_CAP][WARP_KERNEL_WARPS];
+    __shared__ int si[WARP_KERNEL_CAP][WARP_KERNEL_WARPS];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    SmemRing<double, WARP_KERNEL_CAP, WARP_KERNEL_WARPS> ring{ se, sv, si, nullptr, wib };
     Ctr ctr = { 0, 0, 0, 0, 0, 0, 0 };
-    unsigned pts = 0;
+    unsigned pts = 0, heavy = 0;
     int maxr = 0;
-    const int n = *A.slow_count;
-    const int nthreads = gridDim.x * blockDim.x;
-    const int rounds = (n + nthreads - 1) / nthreads;
-    for (int rd = 0; rd < rounds; ++rd) {
-        int t = rd * nthreads + tid;
-        const bool act = t < n && tid < scratch_items;
-        int pid = act ? A.slow_list[t] : -1;
-        int slot = act ? A.slot_of[pid] : -1;
-        const SetDesc S = A.sets[(act && A.set_of) ? A.set_of[slot] : 0];
-        double2 p = act ? A.spos[slot] : make_double2(0.0, 0.0);
-        SlowRow<double> &row = scratch[tid < scratch_items ? tid : 0];
-        GlobalRing<double, SLOW_CAP> ring{ row.e, row.v, row.id };
-        Builder<double, true, GlobalRing<double, SLOW_CAP>> b(A, S, ring, ctr, p, slot);
-        int r = b.run(act);
-        if (act) {
+    const int n = min(*A.defer_count, A.npoints);
+    for (int item = blockIdx.x * WARP_KERNEL_WARPS + wib; item < n; item += gridDim.x * WARP_KERNEL_WARPS) {
+        const int e = A.defer_list[item];
+        const int pid = e < 0 ? ~e : e;
+        heavy += e < 0;
+        const int slot = A.slot_of[pid];
+        const SetDesc S = A.sets[A.set_of ? A.set_of[slot] : 0];
+        const double2 p = A.spos[slot];
+        Builder<double, true, SmemRing<double, WARP_KERNEL_CAP, WARP_KERNEL_WARPS>> b(A, S, ring, ctr, p, slot);
+        const int r = coop_run(b, lane);
+        if (lane == 0) {
             pts++;
             if (r == R_OK) {
                 finish(A, pid, ring, b.m, maxr);
             } else {
                 atomicOr(&A.st->err_flags, r == R_CAPACITY ? EF_SLOW_OVERFLOW
-                                          : r == R_UNBOUNDED ? EF_UNBOUNDED
-                                          : r == R_NONCONTIG ? EF_NONCONTIG : EF_EXACT_UNRESOLVED);
+                                          : r == R_UNBOUNDED ? EF_UNBOUNDED : EF_NONCONTIG);
                 A.nn[pid] = 0;
             }
         }
+        __syncwarp();
     }
-    if (pts) atomicAdd(&A.st->exact_points, (unsigned long long)pts);
+    if (lane == 0 && pts) atomicAdd(&A.st->exact_points, (unsigned long long)pts);
+    if (lane == 0 && heavy) atomicAdd(&A.st->heavy_points, (unsigned long long)heavy);
     flush_counters(A, ctr, 0, maxr);
 }
 
-static_assert(sizeof(SlowRow<double>) == SLOW_ROW_BYTES, "slow-path row layout");
-size_t slow_scratch_bytes_per_item(int) { return sizeof(SlowRow<double>); }
+
 
 // ------------------------------------------------------------------ local Delaunay test
 // Flags every point whose fan is not certainly a piece of the Delaunay triangulation:
@@ -766,11 +970,9 @@ cudaError_t launch_build(const RingArgs &a, int mode, int sms, int shape, cudaSt
     }
 }
 
-cudaError_t launch_slow(const RingArgs &a, void *scratch, int scratch_items, int, cudaStream_t s)
+cudaError_t launch_deferred(const RingArgs &a, int sms, cudaStream_t s)
 {
-    int blocks = (scratch_items + 63) / 64;
-    if (blocks < 1) blocks = 1;
-    k_build_slow<<<blocks, 64, 0, s>>>(a, reinterpret_cast<SlowRow<double> *>(scratch), scratch_items);
+    k_build_warp<<<max(sms, 1) * 4, WARP_KERNEL_WARPS * 32, 0, s>>>(a);
     return cudaGetLastError();
 }
 

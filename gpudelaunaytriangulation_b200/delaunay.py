@@ -227,6 +227,11 @@ class DelaunayGPU:
     def setKernelShape(self, shape: int):
         _nat.check(self._L.dgt_set_kernel_shape(self._h, int(shape)), "dgt_set_kernel_shape")
 
+    def setWorkBudget(self, budget: int):
+        """Cells + candidates a point may scan in the thread-per-point kernel before the
+        warp-per-point kernel takes it over (0: every point goes to the warp kernel)."""
+        _nat.check(self._L.dgt_set_work_budget(self._h, int(budget)), "dgt_set_work_budget")
+
     def tuning(self) -> dict:
         cs, sh, cap, blk = ctypes.c_double(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         _nat.check(self._L.dgt_get_tuning(self._h, ctypes.byref(cs), ctypes.byref(sh), ctypes.byref(cap),

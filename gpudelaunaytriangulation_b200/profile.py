@@ -4,7 +4,7 @@
 
 Runs `--reps` global triangulations of n seeded uniform points at unit density (and, with
 --repair, one test-and-repair after a sigma=0.02 displacement), then prints the counters of
-the last call.  Launch order per rep: 6 binning kernels, k_build, k_build_slow.
+the last call.  Launch order per rep: 6 binning kernels, k_build, k_build_warp.
 """
 import argparse
 import json

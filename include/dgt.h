@@ -42,7 +42,7 @@ typedef struct dgt_stats {
     long long tests;           /* circle tests evaluated by the filter stage */
     long long fp32_undecided;  /* tests the float32 filter left open (re-run in float64) */
     long long fp64_undecided;  /* tests float64 left open (resolved by exact arithmetic) */
-    long long exact_points;    /* points re-run on the exact / large-ring path */
+    long long exact_points;    /* deferred points rebuilt by a warp each (float64 + exact, 64-entry ring) */
     long long mismatches;      /* check mode: filter decisions contradicted by float64 */
     long long insertions;      /* ring insertions */
     long long flagged;         /* test-and-repair: points flagged by the local test */
@@ -56,12 +56,13 @@ typedef struct dgt_stats {
     int reserved;
     long long repair_calls;    /* test-and-repair calls completed on the device */
     long long md_step;         /* device step counter used by DGT_STEP_AUTO */
+    long long heavy_points;    /* points rebuilt by the warp-per-point kernel (over the work budget) */
 } dgt_stats;
 
 /* phases timed with CUDA events when timing is on (dgt_set_timing) */
 #define DGT_PHASE_BIN 0        /* cell grid: count, scan, scatter, in-cell order */
 #define DGT_PHASE_BUILD 1      /* one-ring kernel over all points (global triangulation) */
-#define DGT_PHASE_SLOW 2       /* exact / large-ring path */
+#define DGT_PHASE_SLOW 2       /* deferred points: warp-per-point kernel, exact / large-ring path */
 #define DGT_PHASE_TEST 3       /* local Delaunay test (test-and-repair) */
 #define DGT_PHASE_REPAIR 4     /* all repair rounds (test-and-repair) */
 #define DGT_NUM_PHASES 5
@@ -69,7 +70,7 @@ typedef struct dgt_stats {
 /* dgt_stats.error_flags */
 #define DGT_FLAG_UNBOUNDED 1    /* a ring kept a virtual corner after scanning the whole box */
 #define DGT_FLAG_NONCONTIG 2    /* degenerate conflict set (duplicate / cocircular input) */
-#define DGT_FLAG_RING_OVERFLOW 4 /* a ring outgrew the large-ring path (64) */
+#define DGT_FLAG_RING_OVERFLOW 4 /* a ring outgrew the deferred path's 64 entries */
 #define DGT_FLAG_UNRESOLVED 8
 #define DGT_FLAG_BAD_POINTS 16
 /* warning only: some Delaunay circle reached past half the box, where minimum-image
@@ -168,9 +169,14 @@ int dgt_clear_flags(dgt_context *ctx, void *stream);
 
 /* Kernel shape of the one-ring kernel: (ring entries kept on chip, threads per block) =
  * 0: (14, 64) default, 1: (12, 64), 2: (16, 64), 3: (14, 32), 4: (12, 32).  Rings longer than
- * the on-chip capacity continue on the exact / large-ring path, so every shape gives the same
+ * the on-chip capacity continue on the deferred (warp-per-point) path, so every shape gives the same
  * output. */
 int dgt_set_kernel_shape(dgt_context *ctx, int shape);
+/* Work budget (no reference counterpart): cells plus candidates one point may scan in the
+ * thread-per-point kernel before it is handed to the warp-per-point kernel (points on the rim
+ * of dense clusters, whose circles reach over large regions).  Default 4096; 0 sends every
+ * point to the warp-per-point kernel.  Both kernels give the same rings. */
+int dgt_set_work_budget(dgt_context *ctx, int budget);
 int dgt_get_tuning(const dgt_context *ctx, double *cell_size, int *shape, int *ring_capacity, int *block);
 
 /* Autotuner (no reference counterpart): times global triangulations of d_points for cell

@@ -208,6 +208,59 @@ def test_clustered_gaussian_mixture():
     assert np.array_equal(O.canonical(t, k)[:, : t.shape[1]], O.canonical(ref.tri, ref.nn)[:, : t.shape[1]])
 
 
+@pytest.mark.parametrize("case", ["uniform", "lattice", "mixture"])
+def test_warp_per_point_kernel_same_rings(case):
+    # work budget 0 sends every point to the warp-per-point kernel (float64 + exact, shared
+    # ring): its rings must equal the restated reference and the per-thread kernel's
+    if case == "uniform":
+        n = 30000
+        L = float(np.sqrt(n))
+        pts, Lx, Ly = W.uniform_points(n, L, 21), L, L
+    elif case == "lattice":
+        pts, Lx, Ly = W.triangular_lattice(96, 96, 1.0, 1e-4, seed=4)
+    else:
+        pts, L = W.gaussian_mixture(65536, components=64, sigma=2.0, L=256.0, seed=9)
+        Lx = Ly = L
+    n = len(pts)
+    out = {}
+    for budget in (None, 0):
+        d = _dg()(n, 32, 0.0 if case != "uniform" else 1.0, (Lx, Ly))
+        if budget is not None:
+            d.setWorkBudget(budget)
+        P = torch.from_numpy(np.ascontiguousarray(pts)).cuda()
+        tri = torch.zeros(32 * n, dtype=torch.int32, device="cuda")
+        nn = torch.zeros(n, dtype=torch.int32, device="cuda")
+        d.globalDelaunayTriangulation(P, tri, nn)
+        st = d.stats()
+        assert st["error_flags"] == 0, st
+        if budget == 0:
+            assert st["heavy_points"] == n and st["exact_points"] == n
+        out[budget] = host(tri, nn)
+        d.close()
+    (t0, k0), (t1, k1) = out[None], out[0]
+    assert np.array_equal(k0, k1)
+    assert np.array_equal(O.canonical(t0, k0), O.canonical(t1, k1))
+    assert_delaunay(pts, Lx, Ly, t1, k1, scan=(case != "mixture"))
+    if case == "uniform":
+        ref = O.restated_global(pts, Lx, Ly, 1.0, 32)
+        assert np.array_equal(O.canonical(t1, k1), O.canonical(ref.tri, ref.nn)[:, :32])
+
+
+def test_clustered_input_defers_only_long_scans():
+    # 1M-point mixture layout at 1/16 size: rim points go to the warp-per-point kernel
+    pts, L = W.gaussian_mixture(65536, components=64, sigma=2.0, L=256.0, seed=9)
+    n = len(pts)
+    d = _dg()(n, 32, 1.0, (L, L))
+    P = torch.from_numpy(pts).cuda()
+    tri = torch.zeros(32 * n, dtype=torch.int32, device="cuda")
+    nn = torch.zeros(n, dtype=torch.int32, device="cuda")
+    d.globalDelaunayTriangulation(P, tri, nn)
+    st = d.stats()
+    assert st["error_flags"] == 0 and 0 < st["heavy_points"] < n // 4, st
+    t, k = host(tri, nn)
+    assert_delaunay(pts, L, L, t, k, scan=False)
+
+
 def test_box_too_small_is_flagged():
     # 16 tight clusters in a 200-wide box: void circles reach past L/2
     pts, L = W.gaussian_mixture(40000, components=16, sigma=2.0, seed=9)
