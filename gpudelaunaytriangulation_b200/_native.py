@@ -32,7 +32,7 @@ EXPORTED = [
     "dgt_get_stats", "dgt_displace", "dgt_error_string", "dgt_version", "dgt_set_timing",
     "dgt_get_phase_times", "dgt_global_triangulation_noalloc", "dgt_md_step", "dgt_md_graph_create",
     "dgt_md_graph_launch", "dgt_md_graph_destroy", "dgt_clear_flags", "dgt_set_kernel_shape",
-    "dgt_get_tuning", "dgt_autotune", "dgt_set_work_budget",
+    "dgt_get_tuning", "dgt_autotune", "dgt_set_work_budget", "dgt_set_flip_repair",
 ]
 STEP_AUTO = 0xFFFFFFFFFFFFFFFF
 NOALLOC_MAX_POINTS = 65536
@@ -61,10 +61,14 @@ class Stats(ctypes.Structure):
         ("repair_calls", ctypes.c_longlong),
         ("md_step", ctypes.c_longlong),
         ("heavy_points", ctypes.c_longlong),
+        ("flips", ctypes.c_longlong),
+        ("flip_spilled", ctypes.c_longlong),
+        ("flip_rounds", ctypes.c_int),
+        ("reserved2", ctypes.c_int),
     ]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("reserved")}
 
 
 class TuneResult(ctypes.Structure):
@@ -79,7 +83,7 @@ class TuneResult(ctypes.Structure):
     ]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("reserved")}
 
 
 class DgtError(RuntimeError):
@@ -144,6 +148,7 @@ def lib() -> ctypes.CDLL:
     L.dgt_clear_flags.argtypes = [vp, vp]
     L.dgt_set_kernel_shape.argtypes = [vp, ctypes.c_int]
     L.dgt_set_work_budget.argtypes = [vp, ctypes.c_int]
+    L.dgt_set_flip_repair.argtypes = [vp, ctypes.c_int]
     L.dgt_get_tuning.argtypes = [vp, P_D, P_I, P_I, P_I]
     L.dgt_autotune.argtypes = [vp, vp, vp, vp, ctypes.c_int, vp, ctypes.POINTER(TuneResult)]
     L.dgt_global_triangulation_noalloc.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,

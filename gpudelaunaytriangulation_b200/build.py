@@ -16,7 +16,7 @@ CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIBDIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(LIBDIR, "libdgt.so")
-SOURCES = ["dgt_bin.cu", "dgt_ring.cu", "dgt_api.cu", "dgt_noalloc.cu"]
+SOURCES = ["dgt_bin.cu", "dgt_ring.cu", "dgt_flip.cu", "dgt_api.cu", "dgt_noalloc.cu"]
 HEADERS = ["dgt_internal.cuh", "dgt_predicates.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -54,6 +54,9 @@ struct DevBuf {
 constexpr int FIRST_ROUNDS = 3;     // repair rounds launched before the first host check
 constexpr int NEXT_ROUNDS = 2;      // rounds per later batch (each kernel exits at once on an empty list)
 constexpr int ASYNC_ROUNDS = 6;     // rounds of an unsynchronised call (convergence flagged on the device)
+constexpr int FLIP_BATCH = 4;       // flip rounds launched before each host check
+constexpr int MAX_FLIP_ROUNDS = 24; // flip rounds of a checked call before the rest is rebuilt
+constexpr int ASYNC_FLIP_ROUNDS = 6; // flip rounds of an unsynchronised call
 
 }  // namespace
 
@@ -74,7 +77,7 @@ struct dgt_context {
     int total_cells = 0;
     int total_blocks = 0;
     DevBuf d_sets, d_set_of, ccount, cstart, cell_of, rank, sidx, slot_of, spos, bsum, mark, list0, list1,
-        defer_list, st, ctl, bcount;
+        defer_list, st, ctl, bcount, claim, flip0, flip1, quad;
     DevStatus *h_st = nullptr;
     cudaStream_t last_stream = nullptr;
     bool stats_valid = false;
@@ -85,6 +88,8 @@ struct dgt_context {
     int sms = 0;
     int shape = 0;   // kernel shape (ring capacity, block size), see dgt_set_kernel_shape
     int work_budget = DEFAULT_WORK_BUDGET;   // per-point cells + candidates of the per-thread kernel
+    int flip = 1;    // test-and-repair starts with edge flips (0: rebuild every flagged point)
+    int flip_cap = 0;
 };
 
 namespace {
@@ -214,6 +219,13 @@ int alloc_all(dgt_context *c)
     DGT_TRY(c->list0.ensure(sizeof(int) * n));
     DGT_TRY(c->list1.ensure(sizeof(int) * n));
     DGT_TRY(c->defer_list.ensure(sizeof(int) * n));
+    c->flip_cap = 2 * n + 1024;
+    const bool fresh_claim = c->claim.bytes < sizeof(unsigned long long) * (size_t)n;
+    DGT_TRY(c->claim.ensure(sizeof(unsigned long long) * n));
+    if (fresh_claim) DGT_TRY(cudaMemset(c->claim.p, 0, sizeof(unsigned long long) * n));   // below every key
+    DGT_TRY(c->flip0.ensure(sizeof(int2) * (size_t)c->flip_cap));
+    DGT_TRY(c->flip1.ensure(sizeof(int2) * (size_t)c->flip_cap));
+    DGT_TRY(c->quad.ensure(sizeof(int2) * (size_t)c->flip_cap));
     bool fresh_mark = c->mark.bytes < sizeof(int) * (size_t)n || !c->ctl.p;
     DGT_TRY(c->mark.ensure(sizeof(int) * n));
     DGT_TRY(c->ctl.ensure(sizeof(DevCtl)));
@@ -324,6 +336,9 @@ void to_stats(const DevStatus &d, dgt_stats *o)
     o->repaired = (long long)d.repaired;
     o->cells = (long long)d.cells;
     o->heavy_points = (long long)d.heavy_points;
+    o->flips = (long long)d.flips;
+    o->flip_spilled = (long long)d.flip_spilled;
+    o->flip_rounds = d.flip_rounds;
     o->repair_rounds = d.rounds;
     o->max_ring = d.max_ring;
     o->error_flags = d.err_flags;
@@ -432,7 +447,7 @@ void dgt_destroy(dgt_context *c)
     if (!c) return;
     DevBuf *bufs[] = { &c->d_sets, &c->d_set_of, &c->ccount, &c->cstart, &c->cell_of, &c->rank, &c->sidx,
                        &c->slot_of, &c->spos, &c->bsum, &c->mark, &c->list0, &c->list1, &c->defer_list,
-                       &c->st, &c->ctl, &c->bcount };
+                       &c->st, &c->ctl, &c->bcount, &c->claim, &c->flip0, &c->flip1, &c->quad };
     for (DevBuf *b : bufs) b->release();
     if (c->h_st) cudaFreeHost(c->h_st);
     for (int p = 0; p < DGT_NUM_PHASES; ++p)
@@ -506,6 +521,10 @@ int repair_impl(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, i
     t.epoch_ptr = &ctl->epoch;
     t.list = lists[0];
     t.list_count = &dst->list_count[0];
+    int2 *flips[2] = { c->flip0.as<int2>(), c->flip1.as<int2>() };
+    t.flip_list = c->flip ? flips[0] : nullptr;
+    t.flip_count = &dst->flip_count[0];
+    t.flip_cap = c->flip_cap;
     t.st = dst;
     {
         PhaseTimer pt(c, DGT_PHASE_TEST, s);
@@ -513,6 +532,49 @@ int repair_impl(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, i
         DGT_TRY(launch_test(t, s));
     }
     phase_begin(c, DGT_PHASE_REPAIR, s);
+    if (c->flip) {
+        // Lawson flips first; what they cannot settle joins the rebuild list (list 0)
+        FlipArgs f;
+        std::memset(&f, 0, sizeof(f));
+        f.sets = t.sets;
+        f.set_of = t.set_of;
+        f.pos = t.pos;
+        f.tri = d_tri;
+        f.nn = d_nn;
+        f.stride = stride;
+        f.n = c->n;
+        f.mark = t.mark;
+        f.epoch_ptr = &ctl->epoch;
+        f.rebuild_list = lists[0];
+        f.rebuild_count = &dst->list_count[0];
+        f.claim = c->claim.as<unsigned long long>();
+        f.stamp_ptr = &ctl->flip_stamp;
+        f.quad = c->quad.as<int2>();
+        f.cap = c->flip_cap;
+        f.st = dst;
+        int fr = 0;
+        for (;;) {
+            const int batch = fixed_rounds > 0 ? ASYNC_FLIP_ROUNDS : FLIP_BATCH;
+            for (int b = 0; b < batch; ++b, ++fr) {
+                f.cur = flips[fr & 1];
+                f.cur_count = &dst->flip_count[fr & 1];
+                f.next = flips[(fr + 1) & 1];
+                f.next_count = &dst->flip_count[(fr + 1) & 1];
+                DGT_TRY(cudaMemsetAsync(f.next_count, 0, sizeof(int), s));
+                c->launches += 2;
+                DGT_TRY(launch_flip_round(f, fr, c->sms, s));
+            }
+            if (fixed_rounds > 0 || fr >= MAX_FLIP_ROUNDS) break;
+            int left = 0;
+            DGT_TRY(cudaMemcpyAsync(&left, &dst->flip_count[fr & 1], sizeof(int), cudaMemcpyDeviceToHost, s));
+            DGT_TRY(cudaStreamSynchronize(s));
+            if (left == 0) break;
+        }
+        f.cur = flips[fr & 1];
+        f.cur_count = &dst->flip_count[fr & 1];
+        c->launches += 2;
+        DGT_TRY(launch_flip_spill(f, fr, ctl, c->sms, s));
+    }
     int round = 0;
     bool pending = false;
     for (;;) {
@@ -527,6 +589,8 @@ int repair_impl(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, i
             a.worklist_count = &dst->list_count[cur];
             a.n_items = c->n;
             a.repair = 1;
+            // a round that fits one wave of the warp-per-point kernel goes there whole
+            a.warp_items = c->sms * 16;
             a.epoch_ptr = &ctl->epoch;
             a.round = round;
             a.next_list = lists[nxt];
@@ -763,6 +827,13 @@ int dgt_set_kernel_shape(dgt_context *c, int shape)
 {
     if (!c || shape < 0 || shape >= KERNEL_SHAPES) return DGT_ERR_INVALID_ARGUMENT;
     c->shape = shape;
+    return DGT_OK;
+}
+
+int dgt_set_flip_repair(dgt_context *c, int on)
+{
+    if (!c) return DGT_ERR_INVALID_ARGUMENT;
+    c->flip = on ? 1 : 0;
     return DGT_OK;
 }
 

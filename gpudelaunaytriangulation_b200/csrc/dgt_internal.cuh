@@ -52,6 +52,7 @@ struct DevStatus {
     int rounds;                 // repair rounds executed (device-side count)
     int list_count[2];          // repair work lists (ping-pong)
     int defer_count;            // items queued for the warp-per-point kernel
+    int flip_count[2];          // flip candidate lists (ping-pong)
     int pad;
     unsigned long long points;          // ring constructions
     unsigned long long candidates;      // candidates examined
@@ -66,6 +67,10 @@ struct DevStatus {
     unsigned long long repaired;        // points rebuilt by repair rounds
     unsigned long long cells;           // grid cells scanned
     unsigned long long heavy_points;    // deferred because they outgrew the per-thread work budget
+    unsigned long long flips;           // test-and-repair: edge flips applied
+    unsigned long long flip_spilled;    // flip candidates left after the last flip round
+    int flip_rounds;                    // flip rounds run
+    int pad2;
 };
 
 enum : int {
@@ -87,6 +92,8 @@ struct DevCtl {
     int sticky;                 // error flags of every call since the last reset
     unsigned long long step;    // displacement step counter (dgt_displace with DGT_STEP_AUTO)
     unsigned long long calls;   // test-and-repair calls completed
+    unsigned flip_stamp;        // last flip-round stamp used (claims of later rounds are larger)
+    int pad;
 };
 
 enum : int { MODE_F32 = 0, MODE_F64 = 1 };
@@ -139,6 +146,7 @@ struct RingArgs {
     int *defer_list;
     int *defer_count;
     int work_budget;
+    int warp_items;    // work lists of at most this many items are rebuilt by the warp kernel alone
     int check;         // 1: count float32 decisions contradicted by float64
     DevStatus *st;
 };
@@ -157,6 +165,34 @@ struct TestArgs {
     const int *epoch_ptr;   // this call's base epoch is *epoch_ptr + 1
     int *list;
     int *list_count;
+    // flip mode (flip_list != null): illegal edges (i < j) of valid fans go to the flip list,
+    // invalid fans to the rebuild list
+    int2 *flip_list;
+    int *flip_count;
+    int flip_cap;
+    DevStatus *st;
+};
+
+struct FlipArgs {
+    const SetDesc *sets;
+    const int *set_of;
+    const double2 *pos;
+    int *tri;
+    int *nn;
+    int stride;
+    int n;
+    int *mark;                  // rebuild marks (this call's base epoch is *epoch_ptr + 1)
+    const int *epoch_ptr;
+    int *rebuild_list;          // points for the rebuild rounds
+    int *rebuild_count;
+    unsigned long long *claim;  // per point: (stamp << 32) | slot of the candidate holding it
+    const unsigned *stamp_ptr;  // round r of this call uses stamp *stamp_ptr + 1 + r
+    int2 *cur;                  // candidates (i < j) of this round
+    const int *cur_count;
+    int2 *quad;                 // per candidate: (a, b) when it claimed, (-1, -1) otherwise
+    int2 *next;                 // candidates of the next round
+    int *next_count;
+    int cap;                    // capacity of cur / next / quad
     DevStatus *st;
 };
 
@@ -171,6 +207,9 @@ cudaError_t launch_build(const RingArgs &a, int mode, int sms, int shape, cudaSt
 cudaError_t launch_deferred(const RingArgs &a, int sms, cudaStream_t s);
 constexpr int DEFAULT_WORK_BUDGET = 4096;
 cudaError_t launch_test(const TestArgs &a, cudaStream_t s);
+cudaError_t launch_flip_round(const FlipArgs &a, int round, int sms, cudaStream_t s);
+// leftover candidates to the rebuild list; advances the context's flip stamp by rounds + 1
+cudaError_t launch_flip_spill(const FlipArgs &a, int rounds, DevCtl *ctl, int sms, cudaStream_t s);
 cudaError_t launch_restride(const int *src, int old_stride, int *dst, int new_stride, const int *nn, int n,
                             cudaStream_t s);
 // step_ptr != null: the step comes from (and is advanced in) device memory

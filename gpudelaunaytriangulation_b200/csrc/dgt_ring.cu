@@ -593,6 +593,7 @@ __global__ void __launch_bounds__(BLOCK) k_build(RingArgs A)
     unsigned pts = 0;
     int maxr = 0;
     const int n = item_count(A);
+    if (A.worklist && n <= A.warp_items) return;   // a short work list: k_build_warp takes it
     if (A.repair && blockIdx.x == 0 && threadIdx.x == 0 && n > 0) {
         atomicAdd(&A.st->repaired, (unsigned long long)n);
         atomicMax(&A.st->rounds, A.round + 1);
@@ -635,8 +636,8 @@ __global__ void __launch_bounds__(BLOCK) k_build(RingArgs A)
 // Points the per-thread kernel hands on -- rings longer than its capacity, predicates neither
 // float32 nor float64 decides, and scans longer than the work budget (typically on the rim of
 // dense clusters, where the circles reach over large, partly empty and partly dense regions)
-// -- are rebuilt by a whole warp.  The 32 lanes share one ring in shared memory (float64
-// filter, exact residue, 64 entries), take 32 new cells at a time (dropping empty occupancy
+// -- are rebuilt by a whole warp.  The 32 lanes share one ring in shared memory (float32
+// filter, float64 recheck, exact residue, 64 entries), take 32 new cells at a time (dropping empty occupancy
 // blocks and cells that no current circle reaches) and 32 candidates at a time.  One lane inserts; lanes whose
 // candidates conflicted test them again against the new ring (a candidate outside every
 // circle stays outside, see cell_reached).  The scanned rectangle grows one cell per side
@@ -750,7 +751,7 @@ __device__ int coop_run(B &b, const int lane)
                 }
                 const int sl = __shfl_sync(0xffffffffu, start, o) + j - __shfl_sync(0xffffffffu, excl, o);
                 const bool have = j < total;
-                V2 d = make_double2(0.0, 0.0);
+                V2 d = B::PR::mk2(0, 0);
                 Mask mask = 0;
                 if (have) b.classify(sl, d, mask);
                 unsigned want = __ballot_sync(0xffffffffu, have && mask != 0);
@@ -788,23 +789,31 @@ __device__ int coop_run(B &b, const int lane)
 
 __global__ void __launch_bounds__(WARP_KERNEL_WARPS * 32, 4) k_build_warp(RingArgs A)
 {
-    __shared__ double4 se[WARP_KERNEL_CAP][WARP_KERNEL_WARPS];
-    __shared__ double2 sv[WARP_KERNEL_CAP][WARP_KERNEL_WARPS];
+    __shared__ float4 se[WARP_KERNEL_CAP][WARP_KERNEL_WARPS];
+    __shared__ float2 sv[WARP_KERNEL_CAP][WARP_KERNEL_WARPS];
     __shared__ int si[WARP_KERNEL_CAP][WARP_KERNEL_WARPS];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    SmemRing<double, WARP_KERNEL_CAP, WARP_KERNEL_WARPS> ring{ se, sv, si, nullptr, wib };
+    SmemRing<float, WARP_KERNEL_CAP, WARP_KERNEL_WARPS> ring{ se, sv, si, nullptr, wib };
     Ctr ctr = { 0, 0, 0, 0, 0, 0, 0 };
     unsigned pts = 0, heavy = 0;
     int maxr = 0;
-    const int n = min(*A.defer_count, A.npoints);
+    // a short work list is rebuilt here directly (a warp per point has a far shorter latency
+    // than one thread per point, and few points cannot hide it); otherwise the deferred points
+    const bool direct = A.worklist && item_count(A) <= A.warp_items;
+    const int n = direct ? item_count(A) : min(*A.defer_count, A.npoints);
+    const int *list = direct ? A.worklist : A.defer_list;
+    if (direct && A.repair && blockIdx.x == 0 && threadIdx.x == 0 && n > 0) {
+        atomicAdd(&A.st->repaired, (unsigned long long)n);
+        atomicMax(&A.st->rounds, A.round + 1);
+    }
     for (int item = blockIdx.x * WARP_KERNEL_WARPS + wib; item < n; item += gridDim.x * WARP_KERNEL_WARPS) {
-        const int e = A.defer_list[item];
+        const int e = list[item];
         const int pid = e < 0 ? ~e : e;
         heavy += e < 0;
         const int slot = A.slot_of[pid];
         const SetDesc S = A.sets[A.set_of ? A.set_of[slot] : 0];
         const double2 p = A.spos[slot];
-        Builder<double, true, SmemRing<double, WARP_KERNEL_CAP, WARP_KERNEL_WARPS>> b(A, S, ring, ctr, p, slot);
+        Builder<float, true, SmemRing<float, WARP_KERNEL_CAP, WARP_KERNEL_WARPS>> b(A, S, ring, ctr, p, slot);
         const int r = coop_run(b, lane);
         if (lane == 0) {
             pts++;
@@ -848,11 +857,37 @@ __device__ __forceinline__ void warp_append(int *list, int *count, const int *it
 }
 
 constexpr int TEST_MAX_QUEUE = 24;
+constexpr int TEST_MAX_EDGES = 6;
 
+__device__ __forceinline__ void warp_append_edges(int2 *list, int *count, int cap, const int2 *items, int k,
+                                                  int *overflow)
+{
+    const int lane = threadIdx.x & 31;
+    int incl = k;
+    for (int o = 1; o < 32; o <<= 1) {
+        int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    int total = __shfl_sync(0xffffffffu, incl, 31);
+    int base = 0;
+    if (lane == 31 && total > 0) base = atomicAdd(count, total);
+    base = __shfl_sync(0xffffffffu, base, 31);
+    int off = base + incl - k;
+    *overflow = 0;
+    for (int i = 0; i < k; ++i) {
+        if (off + i < cap) list[off + i] = items[i];
+        else *overflow = 1;
+    }
+}
+
+// Flip mode (A.flip_list set): a valid fan (every triangle strictly CCW, winding once) sends
+// its illegal or undecided spokes (i, P_k) with i < P_k to the flip list (the flip stage
+// decides them exactly); an invalid fan queues its point for rebuilding.
 __global__ void __launch_bounds__(256) k_test(TestArgs A)
 {
     unsigned long long flagged = 0;
     const int ebase = *A.epoch_ptr + 1;
+    const bool flip = A.flip_list != nullptr;
     for (int base = blockIdx.x * blockDim.x; base < A.n; base += gridDim.x * blockDim.x) {
         // points taken in cell order (slot t -> point sidx[t]): the queue a warp appends is a
         // compact patch of cells, which keeps the repair rounds spatially coherent
@@ -860,6 +895,9 @@ __global__ void __launch_bounds__(256) k_test(TestArgs A)
         const int i = (t < A.n && A.sidx) ? A.sidx[t] : t;
         int q[TEST_MAX_QUEUE];
         int nq = 0;
+        int2 ev[TEST_MAX_EDGES];
+        int ne = 0;
+        bool inverted = false;
         if (t < A.n) {
             int m = A.nn[i];
             bool bad = (m < 3 || m > A.stride);
@@ -901,12 +939,23 @@ __global__ void __launch_bounds__(256) k_test(TestArgs A)
                         if (nf < 3) fail_k[nf] = k;
                         nf++;
                     }
+                    inverted |= o <= 0;
+                    if (flip && o > 0 && ic >= 0 && i < row[k]) {
+                        if (ne < TEST_MAX_EDGES) ev[ne] = make_int2(i, row[k]);
+                        ne++;
+                    }
                     prev = cur;
                     cur = nxt;
                 }
                 if (cross != 1) bad = true;
             }
-            if (bad || nf > 0) {
+            if (flip) {
+                // invalid fan (or more illegal spokes than the edge buffer): rebuild the point
+                if (bad || inverted || ne > TEST_MAX_EDGES) {
+                    if (atomicMax(&A.mark[i], ebase) < ebase) q[nq++] = i;
+                    ne = 0;
+                }
+            } else if (bad || nf > 0) {
                 if (atomicMax(&A.mark[i], ebase) < ebase) q[nq++] = i;
                 if (!bad) {
                     // a spoke failure: its quadrilateral; more than three failures: the whole fan
@@ -927,6 +976,14 @@ __global__ void __launch_bounds__(256) k_test(TestArgs A)
             }
         }
         flagged += nq;
+        if (flip) {
+            int overflow = 0;
+            warp_append_edges(A.flip_list, A.flip_count, A.flip_cap, ev, ne, &overflow);
+            if (overflow && atomicMax(&A.mark[i], ebase) < ebase) {
+                q[nq++] = i;   // list full: the point's spokes are settled by rebuilding it
+                flagged++;
+            }
+        }
         warp_append(A.list, A.list_count, q, nq);
     }
     for (int o = 16; o > 0; o >>= 1) flagged += __shfl_down_sync(0xffffffffu, flagged, o);

@@ -227,6 +227,10 @@ class DelaunayGPU:
     def setKernelShape(self, shape: int):
         _nat.check(self._L.dgt_set_kernel_shape(self._h, int(shape)), "dgt_set_kernel_shape")
 
+    def setFlipRepair(self, on: bool):
+        """Test-and-repair by Lawson flips first (default) or by rebuilding every flagged point."""
+        _nat.check(self._L.dgt_set_flip_repair(self._h, int(bool(on))), "dgt_set_flip_repair")
+
     def setWorkBudget(self, budget: int):
         """Cells + candidates a point may scan in the thread-per-point kernel before the
         warp-per-point kernel takes it over (0: every point goes to the warp kernel)."""

@@ -57,6 +57,10 @@ typedef struct dgt_stats {
     long long repair_calls;    /* test-and-repair calls completed on the device */
     long long md_step;         /* device step counter used by DGT_STEP_AUTO */
     long long heavy_points;    /* points rebuilt by the warp-per-point kernel (over the work budget) */
+    long long flips;           /* test-and-repair: edge flips applied */
+    long long flip_spilled;    /* test-and-repair: flip candidates handed to the rebuild rounds */
+    int flip_rounds;           /* test-and-repair: flip rounds run */
+    int reserved2;
 } dgt_stats;
 
 /* phases timed with CUDA events when timing is on (dgt_set_timing) */
@@ -177,6 +181,11 @@ int dgt_set_kernel_shape(dgt_context *ctx, int shape);
  * of dense clusters, whose circles reach over large regions).  Default 4096; 0 sends every
  * point to the warp-per-point kernel.  Both kernels give the same rings. */
 int dgt_set_work_budget(dgt_context *ctx, int budget);
+/* Repair strategy (no reference counterpart): on (default), test-and-repair first flips the
+ * illegal edges of valid fans (Lawson) and rebuilds only what flips cannot settle (inverted
+ * or non-winding fans, inconsistent quadrilaterals); off, it rebuilds every flagged point
+ * and the four points of every failing spoke, as the reference does.  Same result. */
+int dgt_set_flip_repair(dgt_context *ctx, int on);
 int dgt_get_tuning(const dgt_context *ctx, double *cell_size, int *shape, int *ring_capacity, int *block);
 
 /* Autotuner (no reference counterpart): times global triangulations of d_points for cell

@@ -124,7 +124,36 @@ def test_repair_steps_match_fresh_triangulation(sigma, steps):
         assert np.array_equal(k, ref.nn)
         assert np.array_equal(O.canonical(t, k)[:, :16], O.canonical(ref.tri, ref.nn)[:, :16])
         st = d.stats()
-        assert st["flagged"] > 0 and st["repair_rounds"] >= 1 and st["error_flags"] == 0
+        assert st["flagged"] + st["flips"] > 0 and st["error_flags"] == 0
+
+
+@pytest.mark.parametrize("sigma", [0.02, 0.3])
+def test_flip_and_rebuild_repairs_agree(sigma):
+    # flip-first repair (default) and rebuild-only repair (the reference's strategy) must give
+    # the fresh triangulation of the moved points; sigma 0.3 inverts many fans (rebuild path)
+    n = 30000
+    L = float(np.sqrt(n))
+    pts = W.uniform_points(n, L, 53)
+    runs = {}
+    for flip in (True, False):
+        d, P, tri, nn = gpu_build(pts, L, L)
+        d.setFlipRepair(flip)
+        cur = pts
+        for s in range(3):
+            cur = W.displace(cur, sigma, L, L, 700 + s)
+            P.copy_(torch.from_numpy(cur))
+            d.testAndRepairDelaunayTriangulation(P, tri, nn)
+            st = d.stats()
+            assert st["error_flags"] == 0, st
+            if flip:
+                assert st["flips"] > 0, st
+            else:
+                assert st["flips"] == 0 and st["flagged"] > 0, st
+        runs[flip] = host(tri, nn)
+    ref = O.restated_global(cur, L, L, 1.0, 32)
+    for flip, (t, k) in runs.items():
+        assert np.array_equal(k, ref.nn), flip
+        assert np.array_equal(O.canonical(t, k)[:, :16], O.canonical(ref.tri, ref.nn)[:, :16]), flip
 
 
 def test_repair_of_reference_style_local_moves():
