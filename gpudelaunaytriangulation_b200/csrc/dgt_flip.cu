@@ -16,7 +16,8 @@
 // touches a point already queued for rebuilding, and claims its four vertices with a 64-bit
 // atomicMax of (round stamp, mixed list slot); k_flip_apply lets every candidate that holds
 // all four claims flip (winners' quadrilaterals are vertex-disjoint, so no ring is edited
-// twice in a round) and queues the losers and the four outer edges of each flip.  Stamps
+// twice in a round) and queues the losers and those outer edges of each flip that a float32
+// in-circle cannot show legal.  Stamps
 // only grow (a per-context device counter advanced at the end of each call), so claims are
 // never cleared.  Anything the flips cannot settle -- a quadrilateral that is inconsistent
 // between the rings, a ring that would outgrow the stride or shrink below three, offsets
@@ -25,97 +26,11 @@
 // finish the repair.
 #include "dgt_internal.cuh"
 #include "dgt_predicates.cuh"
+#include "dgt_rowreg.cuh"
 
 namespace dgt {
 
 namespace {
-
-// Rings up to RR entries are searched and edited in registers (every index below is a
-// compile-time constant after unrolling); a quadrilateral with a longer ring is rebuilt.
-constexpr int RR = 16;
-
-struct Ring16 {
-    int r[RR];
-};
-
-// the first min(stride, RR) entries of a row (entries past the ring length are ignored by
-// the searches); 16-byte vector loads when the row is aligned and the stride a multiple of 4
-__device__ __forceinline__ void row_load(const int *row, int stride, Ring16 &R)
-{
-    const int lim = stride < RR ? stride : RR;
-    if ((stride & 3) == 0 && (reinterpret_cast<uintptr_t>(row) & 15) == 0) {
-        const int4 *v = reinterpret_cast<const int4 *>(row);
-#pragma unroll
-        for (int q = 0; q < RR / 4; ++q) {
-            int4 x = make_int4(-1, -1, -1, -1);
-            if (4 * q < lim) x = v[q];
-            R.r[4 * q] = x.x;
-            R.r[4 * q + 1] = x.y;
-            R.r[4 * q + 2] = x.z;
-            R.r[4 * q + 3] = x.w;
-        }
-    } else {
-#pragma unroll
-        for (int t = 0; t < RR; ++t) R.r[t] = t < lim ? row[t] : -1;
-    }
-}
-
-// position of x in the ring of length m (<= RR), with its CCW predecessor and successor
-__device__ __forceinline__ int ring_find(const Ring16 &R, int m, int x, int &pred, int &succ)
-{
-    int k = -1, last = R.r[0];
-#pragma unroll
-    for (int t = 1; t < RR; ++t)
-        if (t == m - 1) last = R.r[t];
-    pred = succ = -1;
-#pragma unroll
-    for (int t = 0; t < RR; ++t) {
-        if (t < m && R.r[t] == x) {
-            k = t;
-            pred = t == 0 ? last : R.r[t > 0 ? t - 1 : 0];
-            succ = t + 1 < m ? R.r[t + 1 < RR ? t + 1 : 0] : R.r[0];
-        }
-    }
-    return k;
-}
-
-// remove position k (ring length m -> m - 1)
-__device__ __forceinline__ void ring_drop(Ring16 &R, int k)
-{
-#pragma unroll
-    for (int t = 0; t < RR - 1; ++t)
-        if (t >= k) R.r[t] = R.r[t + 1];
-}
-
-// insert x right after position k (ring length m < RR -> m + 1)
-__device__ __forceinline__ void ring_put_after(Ring16 &R, int k, int x)
-{
-#pragma unroll
-    for (int t = RR - 1; t > 0; --t)
-        if (t > k + 1) R.r[t] = R.r[t - 1];
-#pragma unroll
-    for (int t = 0; t < RR; ++t)
-        if (t == k + 1) R.r[t] = x;
-}
-
-// write a ring of length w rotated to start at its smallest index
-__device__ __forceinline__ void ring_store(int *row, const Ring16 &R, int w)
-{
-    int best = 0, bv = R.r[0];
-#pragma unroll
-    for (int t = 1; t < RR; ++t)
-        if (t < w && R.r[t] < bv) {
-            bv = R.r[t];
-            best = t;
-        }
-#pragma unroll
-    for (int t = 0; t < RR; ++t)
-        if (t < w) {
-            int d = t - best;
-            if (d < 0) d += w;
-            row[d] = R.r[t];
-        }
-}
 
 __device__ __forceinline__ double2 offset_of(const double2 *pos, double2 p, const SetDesc &S, int id)
 {
@@ -127,6 +42,12 @@ __device__ __forceinline__ double2 offset_of(const double2 *pos, double2 p, cons
 __device__ __noinline__ int incircle_exact_call(double2 a, double2 b, double2 d)
 {
     return incircle_exact(a.x, a.y, b.x, b.y, d.x, d.y);
+}
+
+// float32 offset of q relative to p (minimum image, rounded once in double, then to float)
+__device__ __forceinline__ float2 off32(double2 q, double2 p, const SetDesc &S)
+{
+    return make_float2(__double2float_rn(wrap_off(q.x, p.x, S.Lx, S.hLx)), __double2float_rn(wrap_off(q.y, p.y, S.Ly, S.hLy)));
 }
 
 // exact sign of "d strictly inside the circle through (0, a, b)" (CCW (0, a, b))
@@ -284,11 +205,6 @@ __global__ void __launch_bounds__(256, 2) k_flip_apply(FlipArgs A, int round)
             if (A.claim[i] != key || A.claim[j] != key || A.claim[a] != key || A.claim[b] != key) {
                 out[k++] = ed;   // lost a vertex to another flip: next round
             } else {
-                // the outer edges may have become illegal: the next round's claim tests them
-                out[k++] = make_int2(min(i, a), max(i, a));
-                out[k++] = make_int2(min(a, j), max(a, j));
-                out[k++] = make_int2(min(j, b), max(j, b));
-                out[k++] = make_int2(min(b, i), max(b, i));
                 // the four rings in registers (lengths checked by the claim: i, j > 3, a, b < RR)
                 int *wi = A.tri + (size_t)i * A.stride, *wj = A.tri + (size_t)j * A.stride;
                 int *wa = A.tri + (size_t)a * A.stride, *wb = A.tri + (size_t)b * A.stride;
@@ -312,6 +228,25 @@ __global__ void __launch_bounds__(256, 2) k_flip_apply(FlipArgs A, int round)
                 A.nn[a] = ma + 1;
                 A.nn[b] = mb + 1;
                 flips++;
+                // The outer edges (i,a), (i,b) seen from i and (j,a), (j,b) seen from j, with
+                // the vertices across them read off the new rings: queued unless the float32
+                // in-circle says legal outside its error bound (a margin far above the rounding
+                // of offsets to another owner, so the claim's exact test would agree).
+                int x, y, z, w, dummy;
+                ring_find(Ri, mi - 1, a, x, dummy);   // ring(i): x, a, b, y
+                ring_find(Ri, mi - 1, b, dummy, y);
+                ring_find(Rj, mj - 1, a, dummy, z);   // ring(j): w, b, a, z
+                ring_find(Rj, mj - 1, b, w, dummy);
+                const SetDesc S = A.sets[A.set_of ? A.set_of[i] : 0];
+                const double2 pi = __ldg(&A.pos[i]), pj = __ldg(&A.pos[j]), pa = __ldg(&A.pos[a]),
+                              pb = __ldg(&A.pos[b]), px = __ldg(&A.pos[x]), py = __ldg(&A.pos[y]),
+                              pz = __ldg(&A.pos[z]), pw = __ldg(&A.pos[w]);
+                const float2 ia = off32(pa, pi, S), ib = off32(pb, pi, S), ix = off32(px, pi, S), iy = off32(py, pi, S);
+                const float2 ja = off32(pa, pj, S), jb = off32(pb, pj, S), jz = off32(pz, pj, S), jw = off32(pw, pj, S);
+                if (incircle32(ix.x, ix.y, ia.x, ia.y, ib.x, ib.y) >= 0) out[k++] = make_int2(min(i, a), max(i, a));
+                if (incircle32(ia.x, ia.y, ib.x, ib.y, iy.x, iy.y) >= 0) out[k++] = make_int2(min(i, b), max(i, b));
+                if (incircle32(jb.x, jb.y, ja.x, ja.y, jz.x, jz.y) >= 0) out[k++] = make_int2(min(j, a), max(j, a));
+                if (incircle32(jw.x, jw.y, jb.x, jb.y, ja.x, ja.y) >= 0) out[k++] = make_int2(min(j, b), max(j, b));
             }
         }
         warp_push_edges(A, ebase, out, k);

@@ -22,6 +22,7 @@
 // 64-entry ring; k_build_warp).
 #include "dgt_internal.cuh"
 #include "dgt_predicates.cuh"
+#include "dgt_rowreg.cuh"
 
 namespace dgt {
 
@@ -503,10 +504,62 @@ __device__ void finish(const RingArgs &A, int pid, Ring &R, int m, int &maxr)
     const int ep = ebase + A.round;
     maxr = max(maxr, m);
     int *row = A.tri + (size_t)pid * A.stride;
-    if (A.repair) {
+    if (A.repair && m <= RR) {
         // consistency of the rebuilt ring with the rings it touches (see enqueue rules in
         // dgt_api.cu: points rebuilt in this call are exact; an untouched point must either
-        // list pid with the matching neighbours on both sides or be rebuilt too)
+        // list pid with the matching neighbours on both sides or be rebuilt too).  Register
+        // form: the old row, the neighbours' marks and ring lengths are loaded at once, each
+        // neighbour row with one vector load.
+        const int om = A.nn[pid];
+        Ring16 old, nb;
+        row_load(row, A.stride, old);
+#pragma unroll
+        for (int k = 0; k < RR; ++k) nb.r[k] = k < m ? R.idx(k) : -1;
+        int mk[RR], mn[RR];
+#pragma unroll
+        for (int k = 0; k < RR; ++k) {
+            mk[k] = k < m ? A.mark[nb.r[k]] : ebase;
+            mn[k] = k < m ? A.nn[nb.r[k]] : 0;
+        }
+        if (om >= 1 && om <= min(A.stride, RR)) {
+#pragma unroll
+            for (int k = 0; k < RR; ++k) {
+                const int o = old.r[k];
+                bool kept = k >= om;
+#pragma unroll
+                for (int t = 0; t < RR; ++t) kept |= (t < m && nb.r[t] == o);
+                if (!kept && o >= 0 && o < A.npoints) enqueue_next(A, ebase, ep, o);
+            }
+        } else if (om >= 1 && om <= A.stride) {
+            for (int k = 0; k < om; ++k) {
+                const int o = row[k];
+                bool kept = false;
+                for (int t = 0; t < m; ++t) kept |= (R.idx(t) == o);
+                if (!kept && o >= 0 && o < A.npoints) enqueue_next(A, ebase, ep, o);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < RR; ++k) {
+            if (k >= m || mk[k] >= ebase) continue;
+            const int pred = k == 0 ? R.idx(m - 1) : nb.r[k > 0 ? k - 1 : 0];
+            const int succ = k + 1 < m ? nb.r[k + 1 < RR ? k + 1 : 0] : nb.r[0];
+            bool ok = mn[k] >= 3 && mn[k] <= min(A.stride, RR);
+            if (ok) {
+                Ring16 rn;
+                row_load(A.tri + (size_t)nb.r[k] * A.stride, A.stride, rn);
+                int pr, sc;
+                ok = ring_find(rn, mn[k], pid, pr, sc) >= 0 && pr == succ && sc == pred;
+            } else if (mn[k] >= 3 && mn[k] <= A.stride) {
+                const int *rr = A.tri + (size_t)nb.r[k] * A.stride;
+                const int l = mn[k];
+                int pos = -1;
+                for (int t = 0; t < l; ++t)
+                    if (rr[t] == pid) pos = t;
+                ok = pos >= 0 && rr[pos == 0 ? l - 1 : pos - 1] == succ && rr[pos + 1 == l ? 0 : pos + 1] == pred;
+            }
+            if (!ok) enqueue_next(A, ebase, ep, nb.r[k]);
+        }
+    } else if (A.repair) {
         int om = A.nn[pid];
         if (om >= 1 && om <= A.stride) {
             for (int k = 0; k < om; ++k) {
@@ -880,6 +933,29 @@ __device__ __forceinline__ void warp_append_edges(int2 *list, int *count, int ca
     }
 }
 
+// One spoke (p, P_k) of a fan: triangle (p, P_k, P_k+1) strictly CCW and P_k+1 outside the
+// circle through (p, P_k-1, P_k); counts the winding crossing and records failures
+__device__ __forceinline__ void test_spoke(double2 prev, double2 cur, double2 nxt, int k, int rk, int i, bool flip,
+                                           int &cross, int &nf, int *fail_k, bool &inverted, int2 *ev, int &ne)
+{
+    int o = orient32(__double2float_rn(cur.x), __double2float_rn(cur.y), __double2float_rn(nxt.x),
+                     __double2float_rn(nxt.y));
+    if (o == 0) o = orient64(cur.x, cur.y, nxt.x, nxt.y);
+    int ic = incircle32(__double2float_rn(prev.x), __double2float_rn(prev.y), __double2float_rn(cur.x),
+                        __double2float_rn(cur.y), __double2float_rn(nxt.x), __double2float_rn(nxt.y));
+    if (ic == 0) ic = incircle64(prev.x, prev.y, cur.x, cur.y, nxt.x, nxt.y);
+    if (cur.y < 0.0 && nxt.y >= 0.0) cross++;
+    if (o <= 0 || ic >= 0) {
+        if (nf < 3) fail_k[nf] = k;
+        nf++;
+    }
+    inverted |= o <= 0;
+    if (flip && o > 0 && ic >= 0 && i < rk) {
+        if (ne < TEST_MAX_EDGES) ev[ne] = make_int2(i, rk);
+        ne++;
+    }
+}
+
 // Flip mode (A.flip_list set): a valid fan (every triangle strictly CCW, winding once) sends
 // its illegal or undecided spokes (i, P_k) with i < P_k to the flip list (the flip stage
 // decides them exactly); an invalid fan queues its point for rebuilding.
@@ -891,8 +967,10 @@ __global__ void __launch_bounds__(256) k_test(TestArgs A)
     for (int base = blockIdx.x * blockDim.x; base < A.n; base += gridDim.x * blockDim.x) {
         // points taken in cell order (slot t -> point sidx[t]): the queue a warp appends is a
         // compact patch of cells, which keeps the repair rounds spatially coherent
+        // flip mode: index order (rows, ring lengths and owner positions stream contiguously;
+        // only the neighbour gathers are random)
         const int t = base + threadIdx.x;
-        const int i = (t < A.n && A.sidx) ? A.sidx[t] : t;
+        const int i = (t < A.n && A.sidx && !flip) ? A.sidx[t] : t;
         int q[TEST_MAX_QUEUE];
         int nq = 0;
         int2 ev[TEST_MAX_EDGES];
@@ -909,45 +987,32 @@ __global__ void __launch_bounds__(256) k_test(TestArgs A)
                     int r = row[k];
                     if (r < 0 || r >= A.n || r == i) bad = true;
                 }
-            }
-            if (!bad) {
+                if (!bad) {
                 const SetDesc S = A.sets[A.set_of ? A.set_of[i] : 0];
-                double2 p = A.sidx ? A.spos[t] : A.pos[i];
+                double2 p = (A.sidx && !flip) ? A.spos[t] : A.pos[i];
                 double2 q0 = __ldg(&A.pos[row[0]]), ql = __ldg(&A.pos[row[m - 1]]);
                 double2 o0 = make_double2(wrap_off(q0.x, p.x, S.Lx, S.hLx), wrap_off(q0.y, p.y, S.Ly, S.hLy));
                 double2 prev = make_double2(wrap_off(ql.x, p.x, S.Lx, S.hLx), wrap_off(ql.y, p.y, S.Ly, S.hLy));
                 double2 cur = o0;
                 int cross = 0;
+                // neighbour positions gathered two spokes ahead of their use
+                double2 qa = __ldg(&A.pos[row[1 < m ? 1 : 0]]), qb = __ldg(&A.pos[row[2 < m ? 2 : 0]]);
                 for (int k = 0; k < m; ++k) {
+                    const double2 qn = qa;
+                    qa = qb;
+                    if (k + 3 < m) qb = __ldg(&A.pos[row[k + 3]]);
                     double2 nxt;
                     if (k + 1 < m) {
-                        double2 qn = __ldg(&A.pos[row[k + 1]]);
                         nxt = make_double2(wrap_off(qn.x, p.x, S.Lx, S.hLx), wrap_off(qn.y, p.y, S.Ly, S.hLy));
                     } else {
                         nxt = o0;
                     }
-                    // triangle (p, P_k, P_k+1) strictly CCW
-                    int o = orient32(__double2float_rn(cur.x), __double2float_rn(cur.y), __double2float_rn(nxt.x),
-                                     __double2float_rn(nxt.y));
-                    if (o == 0) o = orient64(cur.x, cur.y, nxt.x, nxt.y);
-                    // spoke (p, P_k): P_k+1 outside circle (p, P_k-1, P_k)
-                    int ic = incircle32(__double2float_rn(prev.x), __double2float_rn(prev.y), __double2float_rn(cur.x),
-                                        __double2float_rn(cur.y), __double2float_rn(nxt.x), __double2float_rn(nxt.y));
-                    if (ic == 0) ic = incircle64(prev.x, prev.y, cur.x, cur.y, nxt.x, nxt.y);
-                    if (cur.y < 0.0 && nxt.y >= 0.0) cross++;
-                    if (o <= 0 || ic >= 0) {
-                        if (nf < 3) fail_k[nf] = k;
-                        nf++;
-                    }
-                    inverted |= o <= 0;
-                    if (flip && o > 0 && ic >= 0 && i < row[k]) {
-                        if (ne < TEST_MAX_EDGES) ev[ne] = make_int2(i, row[k]);
-                        ne++;
-                    }
+                    test_spoke(prev, cur, nxt, k, row[k], i, flip, cross, nf, fail_k, inverted, ev, ne);
                     prev = cur;
                     cur = nxt;
                 }
                 if (cross != 1) bad = true;
+                }
             }
             if (flip) {
                 // invalid fan (or more illegal spokes than the edge buffer): rebuild the point
