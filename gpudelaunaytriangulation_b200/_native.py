@@ -64,7 +64,7 @@ class Stats(ctypes.Structure):
         ("flips", ctypes.c_longlong),
         ("flip_spilled", ctypes.c_longlong),
         ("flip_rounds", ctypes.c_int),
-        ("reserved2", ctypes.c_int),
+        ("rebinned", ctypes.c_int),
     ]
 
     def as_dict(self):

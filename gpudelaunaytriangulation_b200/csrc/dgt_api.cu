@@ -89,6 +89,7 @@ struct dgt_context {
     int shape = 0;   // kernel shape (ring capacity, block size), see dgt_set_kernel_shape
     int work_budget = DEFAULT_WORK_BUDGET;   // per-point cells + candidates of the per-thread kernel
     int flip = 1;    // test-and-repair starts with edge flips (0: rebuild every flagged point)
+    bool binned = false;   // the cell lists hold a binning of the current grid
     int flip_cap = 0;
 };
 
@@ -245,6 +246,7 @@ int init_context(dgt_context *c)
         cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device);
         if (c->sms <= 0) c->sms = 148;
     }
+    c->binned = false;
     int r = plan_grid(c);
     if (r != DGT_OK) return r;
     return alloc_all(c);
@@ -268,6 +270,7 @@ BinArgs bin_args(dgt_context *c, const double *pts)
     a.spos = c->spos.as<double2>();
     a.block_sums = c->bsum.as<int>();
     a.deterministic = c->deterministic;
+    a.cond = nullptr;
     return a;
 }
 
@@ -279,7 +282,27 @@ cudaError_t run_bin(dgt_context *c, const double *pts, cudaStream_t s)
     e = cudaMemsetAsync(c->bcount.p, 0, sizeof(int) * ((size_t)c->total_blocks + 1), s);
     if (e != cudaSuccess) return e;
     c->launches += (c->n > 0 ? 2 : 0) + 3 + (c->deterministic && c->total_cells > 0 ? 1 : 0);
-    return launch_bin_st(bin_args(c, pts), c->st.as<DevStatus>(), s);
+    e = launch_bin_st(bin_args(c, pts), c->st.as<DevStatus>(), s);
+    if (e == cudaSuccess) c->binned = true;
+    return e;
+}
+
+// Binning for a repair when the context holds a binning of this grid: refresh the
+// cell-order positions and rebin only if some point lies more than MAX_SKIN_CELLS cells
+// outside the cell that lists it (decided on the device).
+cudaError_t run_bin_refresh(dgt_context *c, const double *pts, cudaStream_t s)
+{
+    PhaseTimer t(c, DGT_PHASE_BIN, s);
+    DevStatus *st = c->st.as<DevStatus>();
+    BinArgs a = bin_args(c, pts);
+    cudaError_t e = launch_refresh(a, st, MAX_SKIN_CELLS, s);
+    if (e != cudaSuccess) return e;
+    a.cond = &st->rebin;
+    e = launch_clear_counts(c->ccount.as<int>(), c->total_cells + 1, c->bcount.as<int>(), c->total_blocks + 1,
+                            a.cond, s);
+    if (e != cudaSuccess) return e;
+    c->launches += (c->n > 0 ? 5 : 3) + 3 + (c->deterministic && c->total_cells > 0 ? 1 : 0);
+    return launch_bin_st(a, st, s);
 }
 
 RingArgs ring_args(dgt_context *c, const double *pts, int *tri, int *nn, int stride)
@@ -302,6 +325,7 @@ RingArgs ring_args(dgt_context *c, const double *pts, int *tri, int *nn, int str
     a.mark = c->mark.as<int>();
     a.defer_list = c->defer_list.as<int>();
     a.defer_count = &c->st.as<DevStatus>()->defer_count;
+    a.skin = &c->st.as<DevStatus>()->skin;
     a.work_budget = c->work_budget;
     a.check = c->check;
     a.st = c->st.as<DevStatus>();
@@ -339,6 +363,7 @@ void to_stats(const DevStatus &d, dgt_stats *o)
     o->flips = (long long)d.flips;
     o->flip_spilled = (long long)d.flip_spilled;
     o->flip_rounds = d.flip_rounds;
+    o->rebinned = d.rebin;
     o->repair_rounds = d.rounds;
     o->max_ring = d.max_ring;
     o->error_flags = d.err_flags;
@@ -505,7 +530,13 @@ int repair_impl(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, i
     DevStatus *dst = c->st.as<DevStatus>();
     DevCtl *ctl = c->ctl.as<DevCtl>();
     DGT_TRY(cudaMemsetAsync(c->st.p, 0, sizeof(DevStatus), s));
-    DGT_TRY(run_bin(c, d_points, s));
+    // With the cell lists of an earlier binning of this grid, flip mode measures how far the
+    // points left their cells in the local test and decides on rebinning only once the rebuild rounds
+    // need the lists (they read candidate positions through the index, so the cell-order copy
+    // needs no refresh); rebuild-only mode refreshes it first (its test runs in cell order).
+    const bool fold = c->flip && c->binned;
+    if (!c->binned) DGT_TRY(run_bin(c, d_points, s));
+    else if (!fold) DGT_TRY(run_bin_refresh(c, d_points, s));
     int *lists[2] = { c->list0.as<int>(), c->list1.as<int>() };
     TestArgs t;
     t.sets = c->d_sets.as<SetDesc>();
@@ -525,6 +556,7 @@ int repair_impl(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, i
     t.flip_list = c->flip ? flips[0] : nullptr;
     t.flip_count = &dst->flip_count[0];
     t.flip_cap = c->flip_cap;
+    t.rcell_of = fold ? c->cell_of.as<int>() : nullptr;
     t.st = dst;
     {
         PhaseTimer pt(c, DGT_PHASE_TEST, s);
@@ -575,6 +607,17 @@ int repair_impl(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, i
         c->launches += 2;
         DGT_TRY(launch_flip_spill(f, fr, ctl, c->sms, s));
     }
+    if (fold) {
+        // timed as the bin phase (inside the repair phase's span)
+        PhaseTimer bt(c, DGT_PHASE_BIN, s);
+        DGT_TRY(launch_rebin_decide(dst, MAX_SKIN_CELLS, s));
+        BinArgs a = bin_args(c, d_points);
+        a.cond = &dst->rebin;
+        DGT_TRY(launch_clear_counts(c->ccount.as<int>(), c->total_cells + 1, c->bcount.as<int>(), c->total_blocks + 1,
+                                    a.cond, s));
+        DGT_TRY(launch_bin_st(a, dst, s));
+        c->launches += 2 + (c->n > 0 ? 2 : 0) + 3 + (c->deterministic && c->total_cells > 0 ? 1 : 0);
+    }
     int round = 0;
     bool pending = false;
     for (;;) {
@@ -589,6 +632,7 @@ int repair_impl(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, i
             a.worklist_count = &dst->list_count[cur];
             a.n_items = c->n;
             a.repair = 1;
+            a.cand_by_index = 1;
             // a round that fits one wave of the warp-per-point kernel goes there whole
             a.warp_items = c->sms * 16;
             a.epoch_ptr = &ctl->epoch;

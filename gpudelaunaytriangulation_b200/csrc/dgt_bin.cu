@@ -7,6 +7,13 @@
 //   order    points of a cell sorted by index, so the cell order (and every candidate order
 //            derived from it) is independent of atomic arrival order
 // No host round trip: capacity is exact by construction.
+//
+// Repair without rebinning: the cell lists of the last binning stay valid as candidate
+// lists while no point lies more than half a cell outside the cell that lists it; the ring
+// kernels then read candidate positions through the index and widen certification by that
+// distance.
+// Every binning kernel takes a device-side condition, so deciding needs no host round trip
+// (and a captured graph replays the decision).
 #include "dgt_internal.cuh"
 
 namespace dgt {
@@ -19,8 +26,22 @@ __device__ __forceinline__ int cell_index(const SetDesc &S, double2 p)
     return S.cell_base + cy * S.xsize + cx;
 }
 
+__device__ __forceinline__ bool skip(const int *cond) { return cond && *cond == 0; }
+
+// the zeroed counters a binning starts from (replaces two memsets when the binning is
+// conditional)
+__global__ void __launch_bounds__(256) k_clear_counts(int *ccount, int ncell, int *bcount, int nblock, const int *cond)
+{
+    if (skip(cond)) return;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < ncell || k < nblock; k += gridDim.x * blockDim.x) {
+        if (k < ncell) ccount[k] = 0;
+        if (k < nblock) bcount[k] = 0;
+    }
+}
+
 __global__ void __launch_bounds__(256) k_count(BinArgs a, DevStatus *st)
 {
+    if (skip(a.cond)) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     const SetDesc &S = a.sets[a.set_of ? a.set_of[i] : 0];
@@ -67,8 +88,9 @@ __device__ __forceinline__ int block_exclusive(int v, int *wsum, int *total)
     return r;
 }
 
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan_reduce(const int *in, int n, int *bsum)
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_reduce(const int *in, int n, int *bsum, const int *cond)
 {
+    if (skip(cond)) return;
     __shared__ int wsum[32];
     __shared__ int total;
     int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
@@ -80,8 +102,9 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_reduce(const int *in, int
 }
 
 // single block: exclusive scan of the block sums in place
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan_top(int *bsum, int nb)
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_top(int *bsum, int nb, const int *cond)
 {
+    if (skip(cond)) return;
     __shared__ int wsum[32];
     __shared__ int total;
     int carry = 0;
@@ -105,8 +128,10 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_top(int *bsum, int nb)
     }
 }
 
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(const int *in, int n, const int *bsum, int *out)
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(const int *in, int n, const int *bsum, int *out,
+                                                             const int *cond)
 {
+    if (skip(cond)) return;
     __shared__ int wsum[32];
     __shared__ int total;
     int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
@@ -127,6 +152,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(const int *in, int 
 
 __global__ void __launch_bounds__(256) k_scatter(BinArgs a)
 {
+    if (skip(a.cond)) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     int slot = a.cstart[a.cell_of[i]] + a.rank[i];
@@ -138,6 +164,7 @@ __global__ void __launch_bounds__(256) k_scatter(BinArgs a)
 // per cell: order its points by index (insertion sort; cells hold a handful of points)
 __global__ void __launch_bounds__(256) k_cell_order(BinArgs a)
 {
+    if (skip(a.cond)) return;
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= a.total_cells) return;
     int lo = a.cstart[c], hi = a.cstart[c + 1];
@@ -156,13 +183,47 @@ __global__ void __launch_bounds__(256) k_cell_order(BinArgs a)
     for (int k = lo; k < hi; ++k) a.slot_of[a.sidx[k]] = k;
 }
 
-cudaError_t launch_scan(const int *in, int n, int *bsum, int *out, cudaStream_t s)
+// current positions into cell order; largest distance outside the listing cell (index order:
+// the reads are contiguous, only the cell-order write scatters)
+__global__ void __launch_bounds__(256) k_refresh(BinArgs a, DevStatus *st)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    float mv = 0.0f;
+    if (i < a.n) {
+        const SetDesc &S = a.sets[a.set_of ? a.set_of[i] : 0];
+        double2 p = a.pos[i];
+        if (!(p.x >= 0.0 && p.x < S.Lx && p.y >= 0.0 && p.y < S.Ly)) {
+            atomicOr(&st->err_flags, EF_BAD_INPUT);
+            p = make_double2(0.0, 0.0);
+        }
+        a.spos[a.slot_of[i]] = p;
+        mv = outside_cell(S, a.cell_of[i], p);
+    }
+    for (int o = 16; o > 0; o >>= 1) mv = fmaxf(mv, __shfl_down_sync(0xffffffffu, mv, o));
+    if ((threadIdx.x & 31) == 0 && mv > 0.0f) atomicMax(reinterpret_cast<int *>(&st->skin_measured), __float_as_int(mv));
+}
+
+// non-negative floats order like their bit patterns, hence the integer atomicMax above
+__global__ void k_rebin_decide(DevStatus *st, float max_skin)
+{
+    const float mv = st->skin_measured;
+    const int rebin = !(mv <= max_skin);
+    st->rebin = rebin;
+    st->skin = rebin ? 0.0f : mv;
+}
+
+static cudaError_t launch_scan_c(const int *in, int n, int *bsum, int *out, const int *cond, cudaStream_t s)
 {
     int nb = (n + SCAN_TILE - 1) / SCAN_TILE;
-    k_scan_reduce<<<nb, SCAN_THREADS, 0, s>>>(in, n, bsum);
-    k_scan_top<<<1, SCAN_THREADS, 0, s>>>(bsum, nb);
-    k_scan_apply<<<nb, SCAN_THREADS, 0, s>>>(in, n, bsum, out);
+    k_scan_reduce<<<nb, SCAN_THREADS, 0, s>>>(in, n, bsum, cond);
+    k_scan_top<<<1, SCAN_THREADS, 0, s>>>(bsum, nb, cond);
+    k_scan_apply<<<nb, SCAN_THREADS, 0, s>>>(in, n, bsum, out, cond);
     return cudaGetLastError();
+}
+
+cudaError_t launch_scan(const int *in, int n, int *bsum, int *out, cudaStream_t s)
+{
+    return launch_scan_c(in, n, bsum, out, nullptr, s);
 }
 
 int scan_block_count(int n) { return (n + SCAN_TILE - 1) / SCAN_TILE; }
@@ -171,10 +232,33 @@ int scan_block_count(int n) { return (n + SCAN_TILE - 1) / SCAN_TILE; }
 cudaError_t launch_bin_st(const BinArgs &a, DevStatus *st, cudaStream_t s)
 {
     if (a.n > 0) k_count<<<(a.n + 255) / 256, 256, 0, s>>>(a, st);
-    cudaError_t e = launch_scan(a.ccount, a.total_cells + 1, a.block_sums, a.cstart, s);
+    cudaError_t e = launch_scan_c(a.ccount, a.total_cells + 1, a.block_sums, a.cstart, a.cond, s);
     if (e != cudaSuccess) return e;
     if (a.n > 0) k_scatter<<<(a.n + 255) / 256, 256, 0, s>>>(a);
     if (a.deterministic && a.total_cells > 0) k_cell_order<<<(a.total_cells + 255) / 256, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_refresh(const BinArgs &a, DevStatus *st, float max_skin, cudaStream_t s)
+{
+    if (a.n > 0) k_refresh<<<(a.n + 255) / 256, 256, 0, s>>>(a, st);
+    k_rebin_decide<<<1, 1, 0, s>>>(st, max_skin);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rebin_decide(DevStatus *st, float max_skin, cudaStream_t s)
+{
+    k_rebin_decide<<<1, 1, 0, s>>>(st, max_skin);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_clear_counts(int *ccount, int ncell, int *bcount, int nblock, const int *cond, cudaStream_t s)
+{
+    const int m = ncell > nblock ? ncell : nblock;
+    int blocks = (m + 255) / 256;
+    if (blocks > 4096) blocks = 4096;
+    if (blocks < 1) blocks = 1;
+    k_clear_counts<<<blocks, 256, 0, s>>>(ccount, ncell, bcount, nblock, cond);
     return cudaGetLastError();
 }
 

@@ -44,6 +44,24 @@ inline int set_block_grid(SetDesc &S, int block_base)
     return S.bxsize * S.bysize;
 }
 
+// Distance on a periodic axis of `size` cells from u (cell units) to cell [c, c + 1].
+__device__ __forceinline__ double arc_gap(double u, int c, int size)
+{
+    const double lo = (double)c, hi = lo + 1.0;
+    if (u >= lo && u <= hi) return 0.0;
+    return u < lo ? fmin(lo - u, u + size - hi) : fmin(u - hi, lo + size - u);
+}
+
+// How far, in cells per axis, point p now lies outside the cell c that lists it (0 while
+// inside), rounded up: the margin by which certification must widen while the cell lists
+// are kept (a point strictly inside a circle is listed by a cell within that margin of it).
+__device__ __forceinline__ float outside_cell(const SetDesc &S, int c, double2 p)
+{
+    const int lc = c - S.cell_base, cy = lc / S.xsize, cx = lc - cy * S.xsize;
+    const double g = fmax(arc_gap(p.x * S.icw, cx, S.xsize), arc_gap(p.y * S.ich, cy, S.ysize));
+    return g > 0.0 ? (float)g * 1.0001f + 1e-6f : 0.0f;
+}
+
 // device-side status / counters of one call (zeroed at the start of each call)
 struct DevStatus {
     int need_stride;            // largest ring that did not fit the caller's stride
@@ -70,7 +88,9 @@ struct DevStatus {
     unsigned long long flips;           // test-and-repair: edge flips applied
     unsigned long long flip_spilled;    // flip candidates left after the last flip round
     int flip_rounds;                    // flip rounds run
-    int pad2;
+    int rebin;                          // repair: 1 when this call rebuilt the cell lists
+    float skin_measured;                // repair: largest move since binning, in cells (per axis)
+    float skin;                         // certification margin of this call's rebuilds, in cells
 };
 
 enum : int {
@@ -113,6 +133,7 @@ struct BinArgs {
     double2 *spos;
     int *block_sums;
     int deterministic;
+    const int *cond;    // null: bin; else bin only when *cond != 0 (device-side decision)
 };
 
 struct RingArgs {
@@ -147,6 +168,11 @@ struct RingArgs {
     int *defer_count;
     int work_budget;
     int warp_items;    // work lists of at most this many items are rebuilt by the warp kernel alone
+    // Cell lists older than the positions (repair without rebinning): every point is at most
+    // *skin cells (per axis) from the cell that lists it, so certification widens each
+    // circle's cell rectangle by that much.  Null or 0: the lists are current.
+    const float *skin;
+    int cand_by_index;   // 1: candidate and own positions from pos[] through the index (repair)
     int check;         // 1: count float32 decisions contradicted by float64
     DevStatus *st;
 };
@@ -170,6 +196,9 @@ struct TestArgs {
     int2 *flip_list;
     int *flip_count;
     int flip_cap;
+    // cells of the last binning (index order; null: not measured): how far the points now
+    // lie outside the cells that list them, largest -> st->skin_measured (outside_cell)
+    const int *rcell_of;
     DevStatus *st;
 };
 
@@ -198,6 +227,16 @@ struct FlipArgs {
 
 // launchers (defined in the .cu files)
 cudaError_t launch_bin_st(const BinArgs &a, DevStatus *st, cudaStream_t s);
+// Repair without a full rebin.  The cell lists of the last binning stay usable as candidate
+// lists while no point lies more than MAX_SKIN_CELLS cells outside the cell that lists it:
+// launch_refresh copies the current positions into cell order and measures that distance
+// (st->skin_measured, in cells), launch_rebin_decide sets st->rebin (too far) and st->skin
+// (the margin the ring kernels must add; 0 after a rebin); binning launched with
+// a.cond = &st->rebin then runs only when needed, all decided on the device.
+cudaError_t launch_refresh(const BinArgs &a, DevStatus *st, float max_skin, cudaStream_t s);
+cudaError_t launch_rebin_decide(DevStatus *st, float max_skin, cudaStream_t s);
+cudaError_t launch_clear_counts(int *ccount, int ncell, int *bcount, int nblock, const int *cond, cudaStream_t s);
+constexpr float MAX_SKIN_CELLS = 0.5f;
 cudaError_t launch_scan(const int *in, int n, int *bsum, int *out, cudaStream_t s);
 int scan_block_count(int n);
 constexpr int KERNEL_SHAPES = 5;

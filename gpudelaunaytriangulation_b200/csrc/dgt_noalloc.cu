@@ -173,6 +173,7 @@ extern "C" int dgt_global_triangulation_noalloc(const double *d_points, int n, d
     b.block_sums = reinterpret_cast<int *>(base + OFF_BSUM);
     b.bcount = reinterpret_cast<int *>(base + OFF_BCOUNT);
     b.deterministic = 1;
+    b.cond = nullptr;
     if (launch_bin_st(b, d_st, s) != cudaSuccess) return DGT_ERR_CUDA;
 
     RingArgs r;

@@ -145,7 +145,10 @@ __device__ __noinline__ double4 circle64(const double2 *pos, double2 p, double L
 }
 
 // ------------------------------------------------------------------- the construction
-template <typename T, bool EXACT, class Ring, class C = Ctr>
+// CAND: where candidate positions come from -- 0 the cell-order copy (current after a
+// binning), 1 the caller's positions through the index (repair: the cell lists may be older
+// than the positions), 2 chosen at run time by A.cand_by_index
+template <typename T, bool EXACT, class Ring, class C = Ctr, int CAND = 2>
 struct Builder {
     typedef Prec<T> PR;
     typedef typename PR::T4 E4;
@@ -254,7 +257,10 @@ struct Builder {
     {
         mask = 0;
         if (sl == slot) return R_OK;
-        double2 q = __ldg(&A.spos[sl]);
+        // repair calls read candidates through the index: the cell-order copy may be older
+        // than the positions (cell lists kept from the last binning)
+        const bool by_index = CAND == 1 || (CAND == 2 && A.cand_by_index);
+        double2 q = by_index ? __ldg(&A.pos[__ldg(&A.sidx[sl])]) : __ldg(&A.spos[sl]);
         double2 d64 = make_double2(wrap_off(q.x, p.x, S.Lx, S.hLx), wrap_off(q.y, p.y, S.Ly, S.hLy));
         if (d64.x == 0.0 && d64.y == 0.0) return R_OK;   // coincident point
         ctr.cand++;
@@ -396,8 +402,11 @@ struct Builder {
         }
         // judged on the circles of the latest ring only (the final one when the scan ends)
         minimage = xmin < -S.hLx || xmax > S.hLx || ymin < -S.hLy || ymax > S.hLy;
-        double a0 = fx + xmin * S.icw, a1 = fx + xmax * S.icw;
-        double b0 = fy + ymin * S.ich, b1 = fy + ymax * S.ich;
+        // cell lists older than the positions: a point may sit up to `sk` cells from the cell
+        // that lists it
+        const double sk = A.skin ? (double)*A.skin : 0.0;
+        double a0 = fx + xmin * S.icw - sk, a1 = fx + xmax * S.icw + sk;
+        double b0 = fy + ymin * S.ich - sk, b1 = fy + ymax * S.ich + sk;
         a0 -= 1e-9 * (1.0 + fabs(a0));
         a1 += 1e-9 * (1.0 + fabs(a1));
         b0 -= 1e-9 * (1.0 + fabs(b0));
@@ -419,7 +428,9 @@ struct Builder {
     __device__ bool cell_reached(int rx, int ry, double fx, double fy)
     {
         const double mg = 1e-9;
-        double a0 = (double)rx - fx, a1 = a0 + 1.0, b0 = (double)ry - fy, b1 = b0 + 1.0;
+        const double sk = A.skin ? (double)*A.skin : 0.0;   // see need_rect
+        double a0 = (double)rx - fx - sk, a1 = (double)rx - fx + 1.0 + sk;
+        double b0 = (double)ry - fy - sk, b1 = (double)ry - fy + 1.0 + sk;
         a0 = (a0 - mg * (1.0 + fabs(a0))) * S.cw;
         a1 = (a1 + mg * (1.0 + fabs(a1))) * S.cw;
         b0 = (b0 - mg * (1.0 + fabs(b0))) * S.ch;
@@ -629,8 +640,9 @@ __device__ __forceinline__ int item_count(const RingArgs &A)
     return c < A.n_items ? c : A.n_items;
 }
 
-// hot kernel: shared-memory ring of CAP entries per thread
-template <typename T, int CAP, int BLOCK>
+// hot kernel: shared-memory ring of CAP entries per thread; IDX: candidate and own positions
+// through the index (repair rounds), else from the cell-order copy (global build)
+template <typename T, int CAP, int BLOCK, bool IDX>
 __global__ void __launch_bounds__(BLOCK) k_build(RingArgs A)
 {
     typedef typename Prec<T>::T4 E4;
@@ -666,8 +678,8 @@ __global__ void __launch_bounds__(BLOCK) k_build(RingArgs A)
             }
         }
         const SetDesc S = A.sets[(act && A.set_of) ? __ldg(&A.set_of[slot]) : 0];
-        double2 p = act ? __ldg(&A.spos[slot]) : make_double2(0.0, 0.0);
-        Builder<T, false, SmemRing<T, CAP, BLOCK>, SmemCtr<BLOCK>> b(A, S, ring, ctr, p, slot);
+        double2 p = !act ? make_double2(0.0, 0.0) : (IDX ? __ldg(&A.pos[pid]) : __ldg(&A.spos[slot]));
+        Builder<T, false, SmemRing<T, CAP, BLOCK>, SmemCtr<BLOCK>, IDX ? 1 : 0> b(A, S, ring, ctr, p, slot);
         int r = b.run(act);
         if (act) {
             pts++;
@@ -865,7 +877,7 @@ __global__ void __launch_bounds__(WARP_KERNEL_WARPS * 32, 4) k_build_warp(RingAr
         heavy += e < 0;
         const int slot = A.slot_of[pid];
         const SetDesc S = A.sets[A.set_of ? A.set_of[slot] : 0];
-        const double2 p = A.spos[slot];
+        const double2 p = A.cand_by_index ? A.pos[pid] : A.spos[slot];
         Builder<float, true, SmemRing<float, WARP_KERNEL_CAP, WARP_KERNEL_WARPS>> b(A, S, ring, ctr, p, slot);
         const int r = coop_run(b, lane);
         if (lane == 0) {
@@ -964,6 +976,7 @@ __global__ void __launch_bounds__(256) k_test(TestArgs A)
     unsigned long long flagged = 0;
     const int ebase = *A.epoch_ptr + 1;
     const bool flip = A.flip_list != nullptr;
+    float moved = 0.0f;   // largest distance outside the listing cell (when A.rcell_of is set)
     for (int base = blockIdx.x * blockDim.x; base < A.n; base += gridDim.x * blockDim.x) {
         // points taken in cell order (slot t -> point sidx[t]): the queue a warp appends is a
         // compact patch of cells, which keeps the repair rounds spatially coherent
@@ -976,6 +989,12 @@ __global__ void __launch_bounds__(256) k_test(TestArgs A)
         int2 ev[TEST_MAX_EDGES];
         int ne = 0;
         bool inverted = false;
+        if (t < A.n && A.rcell_of) {
+            const SetDesc S = A.sets[A.set_of ? A.set_of[i] : 0];
+            const double2 p = A.pos[i];
+            if (!(p.x >= 0.0 && p.x < S.Lx && p.y >= 0.0 && p.y < S.Ly)) atomicOr(&A.st->err_flags, EF_BAD_INPUT);
+            moved = fmaxf(moved, outside_cell(S, A.rcell_of[i], p));
+        }
         if (t < A.n) {
             int m = A.nn[i];
             bool bad = (m < 3 || m > A.stride);
@@ -1053,6 +1072,9 @@ __global__ void __launch_bounds__(256) k_test(TestArgs A)
     }
     for (int o = 16; o > 0; o >>= 1) flagged += __shfl_down_sync(0xffffffffu, flagged, o);
     if ((threadIdx.x & 31) == 0 && flagged) atomicAdd(&A.st->flagged, flagged);
+    for (int o = 16; o > 0; o >>= 1) moved = fmaxf(moved, __shfl_down_sync(0xffffffffu, moved, o));
+    if ((threadIdx.x & 31) == 0 && moved > 0.0f)
+        atomicMax(reinterpret_cast<int *>(&A.st->skin_measured), __float_as_int(moved));
 }
 
 // ------------------------------------------------------------------------- launchers
@@ -1067,7 +1089,8 @@ static cudaError_t launch_build_t(const RingArgs &a, int sms, cudaStream_t s)
         blocks = (a.n_items + BLOCK - 1) / BLOCK;
     }
     if (blocks < 1) blocks = 1;
-    k_build<T, CAP, BLOCK><<<blocks, BLOCK, 0, s>>>(a);
+    if (a.cand_by_index) k_build<T, CAP, BLOCK, true><<<blocks, BLOCK, 0, s>>>(a);
+    else k_build<T, CAP, BLOCK, false><<<blocks, BLOCK, 0, s>>>(a);
     return cudaGetLastError();
 }
 

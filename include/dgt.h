@@ -60,7 +60,9 @@ typedef struct dgt_stats {
     long long flips;           /* test-and-repair: edge flips applied */
     long long flip_spilled;    /* test-and-repair: flip candidates handed to the rebuild rounds */
     int flip_rounds;           /* test-and-repair: flip rounds run */
-    int reserved2;
+    int rebinned;              /* test-and-repair: 1 when the call rebuilt the cell lists (a point
+                                  moved more than half a cell since the last binning), 0 when it
+                                  reused them with widened certification */
 } dgt_stats;
 
 /* phases timed with CUDA events when timing is on (dgt_set_timing) */

@@ -127,6 +127,32 @@ def test_repair_steps_match_fresh_triangulation(sigma, steps):
         assert st["flagged"] + st["flips"] > 0 and st["error_flags"] == 0
 
 
+@pytest.mark.parametrize("flip", [True, False], ids=["flips", "rebuild_only"])
+def test_repair_reuses_cell_lists_until_points_drift(flip):
+    # small moves keep the last binning's cell lists (certification widened by the largest
+    # move); once the accumulated move passes half a cell the call rebins; every step must
+    # equal a fresh triangulation
+    n = 30000
+    L = float(np.sqrt(n))
+    pts = W.uniform_points(n, L, 57)
+    d, P, tri, nn = gpu_build(pts, L, L)
+    d.setFlipRepair(flip)
+    cur = pts
+    seen = []
+    for s in range(8):
+        cur = W.displace(cur, 0.06, L, L, 800 + s)
+        P.copy_(torch.from_numpy(cur))
+        d.testAndRepairDelaunayTriangulation(P, tri, nn)
+        st = d.stats()
+        assert st["error_flags"] == 0, st
+        seen.append(st["rebinned"])
+        t, k = host(tri, nn)
+        ref = O.restated_global(cur, L, L, 1.0, 32)
+        assert np.array_equal(k, ref.nn), s
+        assert np.array_equal(O.canonical(t, k)[:, :16], O.canonical(ref.tri, ref.nn)[:, :16]), s
+    assert seen[0] == 0 and 1 in seen, seen
+
+
 @pytest.mark.parametrize("sigma", [0.02, 0.3])
 def test_flip_and_rebuild_repairs_agree(sigma):
     # flip-first repair (default) and rebuild-only repair (the reference's strategy) must give
