@@ -427,10 +427,15 @@ struct Builder {
     // at the cell's vertices, because d - c, |d - c|^2 - |p - c|^2 is affine in c).
     __device__ bool cell_reached(int rx, int ry, double fx, double fy)
     {
+        return rect_reached(rx, rx, ry, ry, fx, fy);
+    }
+    // the same for the cells [rx0, rx1] x [ry0, ry1] together
+    __device__ bool rect_reached(int rx0, int rx1, int ry0, int ry1, double fx, double fy)
+    {
         const double mg = 1e-9;
         const double sk = A.skin ? (double)*A.skin : 0.0;   // see need_rect
-        double a0 = (double)rx - fx - sk, a1 = (double)rx - fx + 1.0 + sk;
-        double b0 = (double)ry - fy - sk, b1 = (double)ry - fy + 1.0 + sk;
+        double a0 = (double)rx0 - fx - sk, a1 = (double)rx1 - fx + 1.0 + sk;
+        double b0 = (double)ry0 - fy - sk, b1 = (double)ry1 - fy + 1.0 + sk;
         a0 = (a0 - mg * (1.0 + fabs(a0))) * S.cw;
         a1 = (a1 + mg * (1.0 + fabs(a1))) * S.cw;
         b0 = (b0 - mg * (1.0 + fabs(b0))) * S.ch;
@@ -745,56 +750,46 @@ __device__ int coop_run(B &b, const int lane)
     bool changed = true;
     int status = R_OK;
     const int max_phase = S.xsize + S.ysize + 8;
-    for (int phase = 0; status == R_OK && phase < max_phase; ++phase) {
-        int nx0 = x0, nx1 = x1, ny0 = y0, ny1 = y1;
-        if (phase == 1) {
-            nx0 = S.xsize >= 3 ? -1 : 0;
-            nx1 = S.xsize >= 2 ? 1 : 0;
-            ny0 = S.ysize >= 3 ? -1 : 0;
-            ny1 = S.ysize >= 2 ? 1 : 0;
-        } else if (phase > 1) {
-            int lx, hx, ly, hy;
-            if (!b.need_rect(fx, fy, lx, hx, ly, hy)) {
-                lx = ly = -(1 << 28);
-                hx = hy = 1 << 28;
+
+    // one candidate per lane (have): classify all, then insert the conflicting ones one at a
+    // time (the others re-test against each new ring)
+    auto settle = [&](int sl, bool have) {
+        V2 d = B::PR::mk2(0, 0);
+        Mask mask = 0;
+        if (have) b.classify(sl, d, mask);
+        unsigned want = __ballot_sync(0xffffffffu, have && mask != 0);
+        while (want) {
+            const int leader = __ffs(want) - 1;
+            int ir = R_OK;
+            if (lane == leader) ir = b.insert(d, __ldg(&A.sidx[sl]), mask);
+            ir = __shfl_sync(0xffffffffu, ir, leader);
+            b.m = __shfl_sync(0xffffffffu, b.m, leader);
+            b.r2max = __shfl_sync(0xffffffffu, b.r2max, leader);
+            __syncwarp();
+            if (ir != R_OK) {
+                status = ir;
+                break;
             }
-            bool real = true;
-            for (int k = 0; k < b.m; ++k) real &= b.R.idx(k) >= 0;
-            const int sx = changed ? 1 : (real ? (1 << 28) : max(1, (x1 - x0 + 1) >> 1));
-            const int sy = changed ? 1 : (real ? (1 << 28) : max(1, (y1 - y0 + 1) >> 1));
-            grow_axis(x0, x1, lx, hx, sx, S.xsize, nx0, nx1);
-            grow_axis(y0, y1, ly, hy, sy, S.ysize, ny0, ny1);
-            if (nx0 == x0 && nx1 == x1 && ny0 == y0 && ny1 == y1) break;
+            changed = true;
+            const bool again = ((want >> lane) & 1u) && lane != leader;
+            mask = 0;
+            if (again) b.classify(sl, d, mask);
+            want = __ballot_sync(0xffffffffu, again && mask != 0);
         }
-        changed = false;
-        // new cells: columns left and right of the old rectangle (nearest first, over its
-        // rows), then rows below and above (over the new columns)
-        const int h = y1 - y0 + 1, w = nx1 - nx0 + 1;
-        const int nl = (x0 - nx0) * h, nr = (nx1 - x1) * h, nb = (y0 - ny0) * w, nt = (ny1 - y1) * w;
-        const int ncell = phase == 0 ? 1 : nl + nr + nb + nt;
+    };
+    // every candidate of the cells [xa, xb] x [ya, yb] (relative to the own cell): 32 cells
+    // at a time, one per lane (empty occupancy blocks dropped, and with `prune` the cells no
+    // current circle reaches), then their candidates 32 at a time
+    auto scan_cells = [&](int xa, int xb, int ya, int yb, bool prune) {
+        const int w = xb - xa + 1, ncell = w * (yb - ya + 1);
         for (int cb = 0; cb < ncell && status == R_OK; cb += 32) {
-            int ci = cb + lane, start = 0, cnt = 0;
+            const int ci = cb + lane;
+            int start = 0, cnt = 0;
             if (ci < ncell) {
-                int rx = 0, ry = 0;
-                if (phase > 0) {
-                    if (ci < nl) {
-                        rx = x0 - 1 - ci / h;
-                        ry = y0 + ci % h;
-                    } else if ((ci -= nl) < nr) {
-                        rx = x1 + 1 + ci / h;
-                        ry = y0 + ci % h;
-                    } else if ((ci -= nr) < nb) {
-                        ry = y0 - 1 - ci / w;
-                        rx = nx0 + ci % w;
-                    } else {
-                        ci -= nb;
-                        ry = y1 + 1 + ci / w;
-                        rx = nx0 + ci % w;
-                    }
-                }
+                const int rx = xa + ci % w, ry = ya + ci / w;
                 const int cx = wrapi(b.ocx + rx, S.xsize), cy = wrapi(b.ocy + ry, S.ysize);
                 const int blk = S.block_base + (cy >> BLOCK_SHIFT) * S.bxsize + (cx >> BLOCK_SHIFT);
-                if (__ldg(&A.bcount[blk]) != 0 && (phase < 2 || b.cell_reached(rx, ry, fx, fy))) {
+                if (__ldg(&A.bcount[blk]) != 0 && (!prune || b.cell_reached(rx, ry, fx, fy))) {
                     const int c = S.cell_base + cy * S.xsize + cx;
                     start = __ldg(&A.cstart[c]);
                     cnt = __ldg(&A.cstart[c + 1]) - start;
@@ -815,28 +810,90 @@ __device__ int coop_run(B &b, const int lane)
                     if (e <= j) o += step;
                 }
                 const int sl = __shfl_sync(0xffffffffu, start, o) + j - __shfl_sync(0xffffffffu, excl, o);
-                const bool have = j < total;
-                V2 d = B::PR::mk2(0, 0);
-                Mask mask = 0;
-                if (have) b.classify(sl, d, mask);
-                unsigned want = __ballot_sync(0xffffffffu, have && mask != 0);
-                while (want) {
-                    const int leader = __ffs(want) - 1;
-                    int ir = R_OK;
-                    if (lane == leader) ir = b.insert(d, __ldg(&A.sidx[sl]), mask);
-                    ir = __shfl_sync(0xffffffffu, ir, leader);
-                    b.m = __shfl_sync(0xffffffffu, b.m, leader);
-                    b.r2max = __shfl_sync(0xffffffffu, b.r2max, leader);
-                    __syncwarp();
-                    if (ir != R_OK) {
-                        status = ir;
-                        break;
+                settle(sl, j < total);
+            }
+        }
+    };
+
+    for (int phase = 0; status == R_OK && phase < max_phase; ++phase) {
+        int nx0 = x0, nx1 = x1, ny0 = y0, ny1 = y1;
+        if (phase == 1) {
+            nx0 = S.xsize >= 3 ? -1 : 0;
+            nx1 = S.xsize >= 2 ? 1 : 0;
+            ny0 = S.ysize >= 3 ? -1 : 0;
+            ny1 = S.ysize >= 2 ? 1 : 0;
+        } else if (phase > 1) {
+            bool real = true;
+            for (int k = 0; k < b.m; ++k) real &= b.R.idx(k) >= 0;
+            int lx, hx, ly, hy;
+            if (!b.need_rect(fx, fy, lx, hx, ly, hy)) {
+                lx = ly = -(1 << 28);
+                hx = hy = 1 << 28;
+            }
+            // one cell per side while the last phase changed the ring; else the extent doubles
+            // (all-real ring) or grows by half (virtual corners left), so each phase
+            // re-derives the rectangle from circles that nearer cells have already shrunk
+            const int sx = changed ? 1 : (real ? max(1, x1 - x0 + 1) : max(1, (x1 - x0 + 1) >> 1));
+            const int sy = changed ? 1 : (real ? max(1, y1 - y0 + 1) : max(1, (y1 - y0 + 1) >> 1));
+            grow_axis(x0, x1, lx, hx, sx, S.xsize, nx0, nx1);
+            grow_axis(y0, y1, ly, hy, sy, S.ysize, ny0, ny1);
+            if (nx0 == x0 && nx1 == x1 && ny0 == y0 && ny1 == y1) break;
+        }
+        changed = false;
+        // new cells: up to four strips (columns left and right of the old rectangle over its
+        // rows, then rows below and above over the new columns); phase 0 is the own cell
+        int sxa[4], sxb[4], sya[4], syb[4];
+        if (phase == 0) {
+            sxa[0] = sxb[0] = sya[0] = syb[0] = 0;
+            for (int q = 1; q < 4; ++q) sxa[q] = 1, sxb[q] = 0, sya[q] = 1, syb[q] = 0;
+        } else {
+            sxa[0] = nx0; sxb[0] = x0 - 1; sya[0] = y0; syb[0] = y1;
+            sxa[1] = x1 + 1; sxb[1] = nx1; sya[1] = y0; syb[1] = y1;
+            sxa[2] = nx0; sxb[2] = nx1; sya[2] = ny0; syb[2] = y0 - 1;
+            sxa[3] = nx0; sxb[3] = nx1; sya[3] = y1 + 1; syb[3] = ny1;
+        }
+        for (int q = 0; q < 4 && status == R_OK; ++q) {
+            const int sw = sxb[q] - sxa[q] + 1, sh = syb[q] - sya[q] + 1;
+            if (sw <= 0 || sh <= 0) continue;
+            if (phase < 2 || sw * sh <= 512) {
+                scan_cells(sxa[q], sxb[q], sya[q], syb[q], phase >= 2);
+                continue;
+            }
+            // a large strip: 8 x 8 tiles first, one per lane; a tile is scanned cell by cell
+            // only when one of the occupancy blocks it touches holds points and its rectangle
+            // meets a current circle (empty space costs one test per tile, not per cell)
+            const int tw = (sw + 7) >> 3, th = (sh + 7) >> 3, ntile = tw * th;
+            for (int tb = 0; tb < ntile && status == R_OK; tb += 32) {
+                const int ti = tb + lane;
+                int ta = 0, tbx = -1, tc = 0, td = -1;
+                bool live = false;
+                if (ti < ntile) {
+                    // nearest tiles first: the left strip from its right edge, the bottom strip
+                    // from its top edge (the others start next to the old rectangle already)
+                    const int ix = q == 0 ? tw - 1 - ti % tw : ti % tw, iy = q == 2 ? th - 1 - ti / tw : ti / tw;
+                    ta = sxa[q] + ix * 8;
+                    tbx = min(ta + 7, sxb[q]);
+                    tc = sya[q] + iy * 8;
+                    td = min(tc + 7, syb[q]);
+                    // occupancy of the (up to 3 x 3) blocks the tile touches
+                    for (int xs = ta; xs <= tbx && !live;) {
+                        const int ax = wrapi(b.ocx + xs, S.xsize), bx = ax >> BLOCK_SHIFT;
+                        const int xe = xs + min((bx + 1) << BLOCK_SHIFT, S.xsize) - ax;   // next block's first x
+                        for (int ys = tc; ys <= td && !live;) {
+                            const int ay = wrapi(b.ocy + ys, S.ysize), by = ay >> BLOCK_SHIFT;
+                            live = __ldg(&A.bcount[S.block_base + by * S.bxsize + bx]) != 0;
+                            ys += min((by + 1) << BLOCK_SHIFT, S.ysize) - ay;
+                        }
+                        xs = xe;
                     }
-                    changed = true;
-                    const bool again = ((want >> lane) & 1u) && lane != leader;
-                    mask = 0;
-                    if (again) b.classify(sl, d, mask);
-                    want = __ballot_sync(0xffffffffu, again && mask != 0);
+                    live = live && b.rect_reached(ta, tbx, tc, td, fx, fy);
+                }
+                unsigned todo = __ballot_sync(0xffffffffu, live);
+                while (todo && status == R_OK) {
+                    const int src = __ffs(todo) - 1;
+                    todo &= todo - 1;
+                    scan_cells(__shfl_sync(0xffffffffu, ta, src), __shfl_sync(0xffffffffu, tbx, src),
+                               __shfl_sync(0xffffffffu, tc, src), __shfl_sync(0xffffffffu, td, src), true);
                 }
             }
         }
