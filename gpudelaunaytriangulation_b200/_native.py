@@ -33,6 +33,7 @@ EXPORTED = [
     "dgt_get_phase_times", "dgt_global_triangulation_noalloc", "dgt_md_step", "dgt_md_graph_create",
     "dgt_md_graph_launch", "dgt_md_graph_destroy", "dgt_clear_flags", "dgt_set_kernel_shape",
     "dgt_get_tuning", "dgt_autotune", "dgt_set_work_budget", "dgt_set_flip_repair",
+    "dgt_validate",
 ]
 STEP_AUTO = 0xFFFFFFFFFFFFFFFF
 NOALLOC_MAX_POINTS = 65536
@@ -69,6 +70,23 @@ class Stats(ctypes.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("reserved")}
+
+
+class Validation(ctypes.Structure):
+    _fields_ = [
+        ("points", ctypes.c_longlong),
+        ("sum_neighbors", ctypes.c_longlong),
+        ("bad_rows", ctypes.c_longlong),
+        ("asymmetric", ctypes.c_longlong),
+        ("not_ccw", ctypes.c_longlong),
+        ("winding", ctypes.c_longlong),
+        ("not_delaunay", ctypes.c_longlong),
+        ("valid", ctypes.c_int),
+        ("reserved", ctypes.c_int),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
 class TuneResult(ctypes.Structure):
@@ -149,6 +167,7 @@ def lib() -> ctypes.CDLL:
     L.dgt_set_kernel_shape.argtypes = [vp, ctypes.c_int]
     L.dgt_set_work_budget.argtypes = [vp, ctypes.c_int]
     L.dgt_set_flip_repair.argtypes = [vp, ctypes.c_int]
+    L.dgt_validate.argtypes = [vp, vp, vp, vp, ctypes.c_int, ctypes.POINTER(Validation), vp]
     L.dgt_get_tuning.argtypes = [vp, P_D, P_I, P_I, P_I]
     L.dgt_autotune.argtypes = [vp, vp, vp, vp, ctypes.c_int, vp, ctypes.POINTER(TuneResult)]
     L.dgt_global_triangulation_noalloc.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,

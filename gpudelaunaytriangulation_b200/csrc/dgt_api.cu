@@ -77,7 +77,7 @@ struct dgt_context {
     int total_cells = 0;
     int total_blocks = 0;
     DevBuf d_sets, d_set_of, ccount, cstart, cell_of, rank, sidx, slot_of, spos, bsum, mark, list0, list1,
-        defer_list, st, ctl, bcount, claim, flip0, flip1, quad;
+        defer_list, st, ctl, bcount, claim, flip0, flip1, quad, vcount;
     DevStatus *h_st = nullptr;
     cudaStream_t last_stream = nullptr;
     bool stats_valid = false;
@@ -472,7 +472,7 @@ void dgt_destroy(dgt_context *c)
     if (!c) return;
     DevBuf *bufs[] = { &c->d_sets, &c->d_set_of, &c->ccount, &c->cstart, &c->cell_of, &c->rank, &c->sidx,
                        &c->slot_of, &c->spos, &c->bsum, &c->mark, &c->list0, &c->list1, &c->defer_list,
-                       &c->st, &c->ctl, &c->bcount, &c->claim, &c->flip0, &c->flip1, &c->quad };
+                       &c->st, &c->ctl, &c->bcount, &c->claim, &c->flip0, &c->flip1, &c->quad, &c->vcount };
     for (DevBuf *b : bufs) b->release();
     if (c->h_st) cudaFreeHost(c->h_st);
     for (int p = 0; p < DGT_NUM_PHASES; ++p)
@@ -871,6 +871,36 @@ int dgt_set_kernel_shape(dgt_context *c, int shape)
 {
     if (!c || shape < 0 || shape >= KERNEL_SHAPES) return DGT_ERR_INVALID_ARGUMENT;
     c->shape = shape;
+    return DGT_OK;
+}
+
+int dgt_validate(dgt_context *c, const double *d_points, const int *d_tri, const int *d_nn, int stride,
+                 dgt_validation *out, void *stream)
+{
+    if (!c || !out) return DGT_ERR_INVALID_ARGUMENT;
+    std::memset(out, 0, sizeof(*out));
+    if (c->n == 0) {
+        out->valid = 1;
+        return DGT_OK;
+    }
+    if (!d_points || !d_tri || !d_nn || !valid_stride(stride)) return DGT_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = (cudaStream_t)stream;
+    DGT_TRY(c->vcount.ensure(sizeof(unsigned long long) * 8));
+    unsigned long long *d = c->vcount.as<unsigned long long>();
+    DGT_TRY(launch_validate(c->d_sets.as<SetDesc>(), c->batch ? c->d_set_of.as<int>() : nullptr,
+                            reinterpret_cast<const double2 *>(d_points), d_tri, d_nn, stride, c->n, d, c->sms, s));
+    unsigned long long h[7];
+    DGT_TRY(cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, s));
+    DGT_TRY(cudaStreamSynchronize(s));
+    out->sum_neighbors = (long long)h[0];
+    out->bad_rows = (long long)h[1];
+    out->asymmetric = (long long)h[2];
+    out->not_ccw = (long long)h[3];
+    out->winding = (long long)h[4];
+    out->not_delaunay = (long long)h[5];
+    out->points = (long long)h[6];
+    out->valid = out->bad_rows == 0 && out->asymmetric == 0 && out->not_ccw == 0 && out->winding == 0 &&
+                 out->not_delaunay == 0 && out->sum_neighbors == 6 * out->points;
     return DGT_OK;
 }
 

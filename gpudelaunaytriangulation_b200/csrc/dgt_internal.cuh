@@ -246,6 +246,9 @@ cudaError_t launch_build(const RingArgs &a, int mode, int sms, int shape, cudaSt
 cudaError_t launch_deferred(const RingArgs &a, int sms, cudaStream_t s);
 constexpr int DEFAULT_WORK_BUDGET = 4096;
 cudaError_t launch_test(const TestArgs &a, cudaStream_t s);
+// device validation counts (sum, bad_rows, asymmetric, not_ccw, winding, not_delaunay, points)
+cudaError_t launch_validate(const SetDesc *sets, const int *set_of, const double2 *pos, const int *tri,
+                            const int *nn, int stride, int n, unsigned long long *out, int sms, cudaStream_t s);
 cudaError_t launch_flip_round(const FlipArgs &a, int round, int sms, cudaStream_t s);
 // leftover candidates to the rebuild list; advances the context's flip stamp by rounds + 1
 cudaError_t launch_flip_spill(const FlipArgs &a, int rounds, DevCtl *ctl, int sms, cudaStream_t s);

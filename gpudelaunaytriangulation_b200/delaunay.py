@@ -227,6 +227,21 @@ class DelaunayGPU:
     def setKernelShape(self, shape: int):
         _nat.check(self._L.dgt_set_kernel_shape(self._h, int(shape)), "dgt_set_kernel_shape")
 
+    def validate(self, points: torch.Tensor, GPUTriangulation: torch.Tensor, cellNeighborNum: torch.Tensor,
+                 stream=None) -> dict:
+        """Check the triangulation on the device (exact predicates): well-formed rows, symmetric
+        rings, counter-clockwise fans winding once, every edge locally Delaunay, ring sizes
+        summing to 6N.  Returns the counts and `valid`."""
+        n = self.Ncells
+        _check_points(points, n)
+        _check_int(GPUTriangulation, "GPUTriangulation")
+        _check_int(cellNeighborNum, "cellNeighborNum")
+        stride = GPUTriangulation.numel() // max(1, n)
+        v = _nat.Validation()
+        _nat.check(self._L.dgt_validate(self._h, _ptr(points), _ptr(GPUTriangulation), _ptr(cellNeighborNum), stride,
+                                        ctypes.byref(v), _stream_ptr(stream)), "dgt_validate")
+        return v.as_dict()
+
     def setFlipRepair(self, on: bool):
         """Test-and-repair by Lawson flips first (default) or by rebuilding every flagged point."""
         _nat.check(self._L.dgt_set_flip_repair(self._h, int(bool(on))), "dgt_set_flip_repair")

@@ -142,6 +142,29 @@ int dgt_restride(const int *d_src, int src_stride, int *d_dst, int dst_stride, c
 /* Counters of the last call (synchronises the context's last stream). */
 int dgt_get_stats(dgt_context *ctx, dgt_stats *out);
 
+/* Device-side validation of a triangulation in the caller's arrays (no reference
+ * counterpart: the reference compares its output with CGAL on the host).  One pass over the
+ * points with exact predicates; every row read is bounds-checked, so corrupt rows are
+ * counted, never followed.  Needs no earlier call on the context besides creation (the
+ * context supplies the box / batched sets); synchronises the stream. */
+typedef struct dgt_validation {
+    long long points;         /* points checked */
+    long long sum_neighbors;  /* sum of all ring lengths (6 * points for a triangulation of the
+                                 torus: 3n edges) */
+    long long bad_rows;       /* length outside [3, stride], index out of range, self or repeated */
+    long long asymmetric;     /* spokes (i, j) where ring(j) lacks i or disagrees on i's two
+                                 adjacent neighbours (the two triangles seen from j) */
+    long long not_ccw;        /* fan triangles (i, P_k, P_k+1) not strictly counter-clockwise */
+    long long winding;        /* fans that do not wind exactly once around their point (or have
+                                 a triangle counted in not_ccw) */
+    long long not_delaunay;   /* spokes whose opposite vertex lies strictly inside the circle
+                                 through the point and its two other neighbours (exact) */
+    int valid;                /* 1: all counts above are 0 and sum_neighbors == 6 * points */
+    int reserved;
+} dgt_validation;
+int dgt_validate(dgt_context *ctx, const double *d_points, const int *d_tri, const int *d_neighnum, int stride,
+                 dgt_validation *out, void *stream);
+
 /* 1: record CUDA events around each phase of every call (on the call's stream). */
 int dgt_set_timing(dgt_context *ctx, int on);
 /* Milliseconds per phase of the last call (DGT_NUM_PHASES values, -1 for phases the call did
