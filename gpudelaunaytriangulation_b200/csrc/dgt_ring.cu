@@ -169,6 +169,11 @@ struct Builder {
     __device__ Builder(const RingArgs &a, const SetDesc &s, Ring &r, C &c, double2 pp, int sl)
         : A(a), S(s), R(r), ctr(c), p(pp), slot(sl), m(0), r2max((T)0), ocx(0), ocy(0) {}
 
+    // r2max bounds |d|^2 for any d inside some edge circle (a circle through the origin of
+    // radius <= rc lies within 2 rc of it): the candidate prefilter.  Exact maximum here;
+    // inserts only fold in their two new circles (still an upper bound: the other circles
+    // are unchanged), and the exact value is restored where the edges are walked anyway.
+    __device__ __forceinline__ static T r2_of(T rc) { return (T)4 * rc * rc * ((T)1 + (T)64 * PR::u()); }
     __device__ void refresh_r2max()
     {
         T mx = (T)0;
@@ -176,7 +181,7 @@ struct Builder {
             T rc = R.edge(k).w;
             mx = rc > mx ? rc : mx;
         }
-        r2max = (T)4 * mx * mx * ((T)1 + (T)64 * PR::u());
+        r2max = r2_of(mx);
     }
 
     // the square of virtual corners (ring storage only)
@@ -247,7 +252,9 @@ struct Builder {
         R.set_edge(ns + 1, cb);
         m = mnew;
         ctr.add_ins();
-        refresh_r2max();
+        const T rn = ca.w > cb.w ? ca.w : cb.w;
+        const T r2n = r2_of(rn);
+        if (!(r2n <= r2max)) r2max = r2n;   // an infinite (unbounded) circle disables the prefilter
         return R_OK;
     }
 
@@ -377,9 +384,13 @@ struct Builder {
     __device__ bool need_rect(double fx, double fy, int &lx, int &hx, int &ly, int &hy)
     {
         double xmin = 1e300, xmax = -1e300, ymin = 1e300, ymax = -1e300;
+        T mx = (T)0;
+        bool finite = true;
         for (int k = 0; k < m; ++k) {
             E4 e = R.edge(k);
             double cx, cy, rc;
+            mx = e.w > mx ? e.w : mx;
+            finite &= e.w < PR::inf();
             if (e.w < PR::inf()) {
                 cx = 0.5 * (double)e.x;
                 cy = 0.5 * (double)e.y;
@@ -400,6 +411,7 @@ struct Builder {
             ymin = fmin(ymin, cy - rc);
             ymax = fmax(ymax, cy + rc);
         }
+        if (finite) r2max = r2_of(mx);   // the exact prefilter bound, restored for free
         // judged on the circles of the latest ring only (the final one when the scan ends)
         minimage = xmin < -S.hLx || xmax > S.hLx || ymin < -S.hLy || ymax > S.hLy;
         // cell lists older than the positions: a point may sit up to `sk` cells from the cell
@@ -469,6 +481,7 @@ struct Builder {
                 live = false;
             }
             if (live && phase == 1) {
+                refresh_r2max();   // after the own cell's insertions
                 // the 3x3 block (fewer columns / rows on grids narrower than 3 cells)
                 gx0 = S.xsize >= 3 ? -1 : 0;
                 gx1 = S.xsize >= 2 ? 1 : 0;
@@ -818,6 +831,7 @@ __device__ int coop_run(B &b, const int lane)
     for (int phase = 0; status == R_OK && phase < max_phase; ++phase) {
         int nx0 = x0, nx1 = x1, ny0 = y0, ny1 = y1;
         if (phase == 1) {
+            b.refresh_r2max();   // after the own cell's insertions (same value on every lane)
             nx0 = S.xsize >= 3 ? -1 : 0;
             nx1 = S.xsize >= 2 ? 1 : 0;
             ny0 = S.ysize >= 3 ? -1 : 0;
