@@ -33,7 +33,7 @@ EXPORTED = [
     "dgt_get_phase_times", "dgt_global_triangulation_noalloc", "dgt_md_step", "dgt_md_graph_create",
     "dgt_md_graph_launch", "dgt_md_graph_destroy", "dgt_clear_flags", "dgt_set_kernel_shape",
     "dgt_get_tuning", "dgt_autotune", "dgt_set_work_budget", "dgt_set_flip_repair",
-    "dgt_validate",
+    "dgt_validate", "dgt_get_cell_order",
 ]
 STEP_AUTO = 0xFFFFFFFFFFFFFFFF
 NOALLOC_MAX_POINTS = 65536
@@ -168,6 +168,7 @@ def lib() -> ctypes.CDLL:
     L.dgt_set_work_budget.argtypes = [vp, ctypes.c_int]
     L.dgt_set_flip_repair.argtypes = [vp, ctypes.c_int]
     L.dgt_validate.argtypes = [vp, vp, vp, vp, ctypes.c_int, ctypes.POINTER(Validation), vp]
+    L.dgt_get_cell_order.argtypes = [vp, vp, vp]
     L.dgt_get_tuning.argtypes = [vp, P_D, P_I, P_I, P_I]
     L.dgt_autotune.argtypes = [vp, vp, vp, vp, ctypes.c_int, vp, ctypes.POINTER(TuneResult)]
     L.dgt_global_triangulation_noalloc.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,

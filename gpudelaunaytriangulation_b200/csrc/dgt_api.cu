@@ -904,6 +904,16 @@ int dgt_validate(dgt_context *c, const double *d_points, const int *d_tri, const
     return DGT_OK;
 }
 
+int dgt_get_cell_order(dgt_context *c, int *d_order, void *stream)
+{
+    if (!c) return DGT_ERR_INVALID_ARGUMENT;
+    if (c->n == 0) return DGT_OK;
+    if (!d_order || !c->binned) return DGT_ERR_INVALID_ARGUMENT;
+    DGT_TRY(cudaMemcpyAsync(d_order, c->sidx.p, sizeof(int) * (size_t)c->n, cudaMemcpyDeviceToDevice,
+                            (cudaStream_t)stream));
+    return DGT_OK;
+}
+
 int dgt_set_flip_repair(dgt_context *c, int on)
 {
     if (!c) return DGT_ERR_INVALID_ARGUMENT;

@@ -242,6 +242,15 @@ class DelaunayGPU:
                                         ctypes.byref(v), _stream_ptr(stream)), "dgt_validate")
         return v.as_dict()
 
+    def cellOrder(self, stream=None) -> torch.Tensor:
+        """Indices of the points in the cell order of the last binning (int32, on the device):
+        renumbering the points in this order puts Delaunay neighbours at nearby indices."""
+        n = self.Ncells
+        out = torch.empty(n, dtype=torch.int32, device="cuda")
+        if n:
+            _nat.check(self._L.dgt_get_cell_order(self._h, _ptr(out), _stream_ptr(stream)), "dgt_get_cell_order")
+        return out
+
     def setFlipRepair(self, on: bool):
         """Test-and-repair by Lawson flips first (default) or by rebuilding every flagged point."""
         _nat.check(self._L.dgt_set_flip_repair(self._h, int(bool(on))), "dgt_set_flip_repair")

@@ -165,6 +165,14 @@ typedef struct dgt_validation {
 int dgt_validate(dgt_context *ctx, const double *d_points, const int *d_tri, const int *d_neighnum, int stride,
                  dgt_validation *out, void *stream);
 
+/* Spatial order of the points (the reference offers a Hilbert-curve pre-pass for the same
+ * purpose, src/utilities/hilbert_curve.cpp; this is the cell order of the last binning):
+ * d_order[k] = index of the k-th point in cell order (cells row-major, points of a cell by
+ * index; for batched contexts set by set).  Renumbering the points in this order puts
+ * Delaunay neighbours at nearby indices.  Needs a global triangulation or test-and-repair on
+ * the context first (DGT_ERR_INVALID_ARGUMENT otherwise); d_order is int[n] on the device. */
+int dgt_get_cell_order(dgt_context *ctx, int *d_order, void *stream);
+
 /* 1: record CUDA events around each phase of every call (on the call's stream). */
 int dgt_set_timing(dgt_context *ctx, int on);
 /* Milliseconds per phase of the last call (DGT_NUM_PHASES values, -1 for phases the call did

@@ -75,3 +75,30 @@ def test_planted_faults_are_counted():
     v = d.validate(P, tri, nn)
     assert v["valid"] == 0 and v["bad_rows"] == 2 and v["asymmetric"] > 0 and v["not_ccw"] > 0, v
     same_as_oracle(v, pts, L, tri, nn)
+
+
+def test_cell_order_renumbering():
+    # the order from the last binning is a permutation along which the cell index never
+    # decreases; triangulating the renumbered points gives the same rings, relabelled
+    n = 30000
+    d, P, tri, nn, pts, L = build(n, 9)
+    order = d.cellOrder().cpu().numpy().astype(np.int64)
+    assert np.array_equal(np.sort(order), np.arange(n))
+    xs = int(np.floor(L / 1.0))
+    cw = L / xs
+    cell = np.minimum(np.floor(pts[order, 1] / cw), xs - 1) * xs + np.minimum(np.floor(pts[order, 0] / cw), xs - 1)
+    assert (np.diff(cell) >= 0).all()
+    d2, P2, tri2, nn2, _, _ = build(n, 9)
+    P2.copy_(torch.from_numpy(np.ascontiguousarray(pts[order])))
+    d2.globalDelaunayTriangulation(P2, tri2, nn2)
+    t2 = tri2.view(n, -1).cpu().numpy()
+    k2 = nn2.cpu().numpy()
+    back = np.full_like(t2, -1)
+    kk = np.zeros(n, np.int32)
+    for new in range(n):
+        back[order[new], : k2[new]] = order[t2[new, : k2[new]]]
+        kk[order[new]] = k2[new]
+    t = tri.view(n, -1).cpu().numpy()
+    k = nn.cpu().numpy()
+    assert np.array_equal(kk, k)
+    assert np.array_equal(O.canonical(back, kk), O.canonical(t, k))
