@@ -32,12 +32,6 @@ namespace dgt {
 
 namespace {
 
-__device__ __forceinline__ double2 offset_of(const double2 *pos, double2 p, const SetDesc &S, int id)
-{
-    double2 q = __ldg(&pos[id]);
-    return make_double2(wrap_off(q.x, p.x, S.Lx, S.hLx), wrap_off(q.y, p.y, S.Ly, S.hLy));
-}
-
 // the exact residue, out of line (its expansion arrays stay off the callers' frames)
 __device__ __noinline__ int incircle_exact_call(double2 a, double2 b, double2 d)
 {
