@@ -33,7 +33,7 @@ EXPORTED = [
     "dgt_get_phase_times", "dgt_global_triangulation_noalloc", "dgt_md_step", "dgt_md_graph_create",
     "dgt_md_graph_launch", "dgt_md_graph_destroy", "dgt_clear_flags", "dgt_set_kernel_shape",
     "dgt_get_tuning", "dgt_autotune", "dgt_set_work_budget", "dgt_set_flip_repair",
-    "dgt_validate", "dgt_get_cell_order",
+    "dgt_validate", "dgt_get_cell_order", "dgt_set_box_general", "dgt_get_box",
 ]
 STEP_AUTO = 0xFFFFFFFFFFFFFFFF
 NOALLOC_MAX_POINTS = 65536
@@ -143,6 +143,8 @@ def lib() -> ctypes.CDLL:
     L.dgt_update_list.argtypes = [vp, vp, vp]
     L.dgt_set_cell_size.argtypes = [vp, ctypes.c_double]
     L.dgt_set_box.argtypes = [vp, ctypes.c_double, ctypes.c_double]
+    L.dgt_set_box_general.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+    L.dgt_get_box.argtypes = [vp, P_D]
     L.dgt_set_safety_mode.argtypes = [vp, ctypes.c_int]
     L.dgt_set_precision.argtypes = [vp, ctypes.c_int]
     L.dgt_set_check_mode.argtypes = [vp, ctypes.c_int]

@@ -67,6 +67,10 @@ struct dgt_context {
     bool batch = false;
     std::vector<int> sizes;
     std::vector<double> boxes;
+    // general periodic box (single-set contexts): the reduced basis the kernels use, columns
+    // (gbox[0], gbox[2]) and (gbox[1], gbox[3]); boxes then holds its bounding rectangle
+    int general = 0;
+    double gbox[4] = { 0, 0, 0, 0 };
     double cell_size = 1.0;
     int max_size = 16;
     int safety = 1;
@@ -152,6 +156,72 @@ double pow2_at_least(double x)
     return v;
 }
 
+// Lagrange-Gauss reduction of a 2D lattice basis (columns (m[0], m[2]) and (m[1], m[3])):
+// afterwards |a| <= |b| and |a.b| <= |a|^2 / 2, the most nearly orthogonal basis of the same
+// lattice.  The periodic Delaunay triangulation depends on the lattice only; a reduced basis
+// makes the fractional minimum image the nearest image for every offset that matters and
+// keeps the cells compact.
+void reduce_basis(double m[4])
+{
+    double ax = m[0], ay = m[2], bx = m[1], by = m[3];
+    for (int it = 0; it < 64; ++it) {
+        if (ax * ax + ay * ay > bx * bx + by * by) {
+            std::swap(ax, bx);
+            std::swap(ay, by);
+        }
+        const double mu = std::nearbyint((ax * bx + ay * by) / (ax * ax + ay * ay));
+        if (mu == 0.0) break;
+        bx -= mu * ax;
+        by -= mu * ay;
+    }
+    m[0] = ax;
+    m[2] = ay;
+    m[1] = bx;
+    m[3] = by;
+}
+
+// general-box fields of a set whose grid is chosen from the cell edge a (see plan_grid)
+void plan_general_set(SetDesc &S, const double m[4], double a, int ns)
+{
+    const double det = m[0] * m[3] - m[1] * m[2];
+    const double area = std::fabs(det);
+    const double la = std::hypot(m[0], m[2]), lb = std::hypot(m[1], m[3]);
+    // the strip between cell lines u = k / xsize is (area / |b|) / xsize wide
+    double amin = std::sqrt(area / (16.0 * std::max(ns, 1) + 64.0));
+    if (a < amin) a = amin;
+    const int xs = std::max(1, (int)std::floor(area / lb / a));
+    const int ys = std::max(1, (int)std::floor(area / la / a));
+    S.general = 1;
+    S.m11 = m[0];
+    S.m12 = m[1];
+    S.m21 = m[2];
+    S.m22 = m[3];
+    S.i11 = m[3] / det;
+    S.i12 = -m[1] / det;
+    S.i21 = -m[2] / det;
+    S.i22 = m[0] / det;
+    S.xsize = xs;
+    S.ysize = ys;
+    S.g11 = xs * S.i11;
+    S.g12 = xs * S.i12;
+    S.g21 = ys * S.i21;
+    S.g22 = ys * S.i22;
+    S.gnx = std::hypot(S.g11, S.g12) * (1.0 + 1e-12);
+    S.gny = std::hypot(S.g21, S.g22) * (1.0 + 1e-12);
+    S.hxs = 0.5 * xs;
+    S.hys = 0.5 * ys;
+    // bounding rectangle (not used for geometry by the general-box kernels)
+    S.Lx = std::fabs(m[0]) + std::fabs(m[1]);
+    S.Ly = std::fabs(m[2]) + std::fabs(m[3]);
+    S.hLx = 0.5 * S.Lx;
+    S.hLy = 0.5 * S.Ly;
+    S.cw = S.Lx / xs;
+    S.ch = S.Ly / ys;
+    S.icw = xs / S.Lx;
+    S.ich = ys / S.Ly;
+    S.V = (float)pow2_at_least(std::max(S.Lx, S.Ly));
+}
+
 // cell grid of every set from the requested cell edge
 int plan_grid(dgt_context *c)
 {
@@ -161,6 +231,19 @@ int plan_grid(dgt_context *c)
     for (int s = 0; s < c->num_sets; ++s) {
         double Lx = c->boxes[2 * s], Ly = c->boxes[2 * s + 1];
         int ns = c->sizes[s];
+        if (c->general) {
+            const double area = std::fabs(c->gbox[0] * c->gbox[3] - c->gbox[1] * c->gbox[2]);
+            SetDesc &S = c->sets[s];
+            plan_general_set(S, c->gbox, c->cell_size > 0 ? c->cell_size : std::sqrt(area / std::max(ns, 1)), ns);
+            S.cell_base = (int)cells;
+            S.point_base = pbase;
+            S.n = ns;
+            blocks += set_block_grid(S, (int)blocks);
+            cells += (long long)S.xsize * S.ysize;
+            pbase += ns;
+            if (cells > (1LL << 30)) return DGT_ERR_INVALID_ARGUMENT;
+            continue;
+        }
         double spacing = std::sqrt(Lx * Ly / std::max(ns, 1));
         double a;
         if (c->batch) a = (c->cell_size > 0 ? c->cell_size : 1.0) * spacing;
@@ -328,6 +411,7 @@ RingArgs ring_args(dgt_context *c, const double *pts, int *tri, int *nn, int str
     a.skin = &c->st.as<DevStatus>()->skin;
     a.work_budget = c->work_budget;
     a.check = c->check;
+    a.general = c->general;
     a.st = c->st.as<DevStatus>();
     return a;
 }
@@ -557,6 +641,7 @@ int repair_impl(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, i
     t.flip_count = &dst->flip_count[0];
     t.flip_cap = c->flip_cap;
     t.rcell_of = fold ? c->cell_of.as<int>() : nullptr;
+    t.general = c->general;
     t.st = dst;
     {
         PhaseTimer pt(c, DGT_PHASE_TEST, s);
@@ -570,6 +655,7 @@ int repair_impl(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, i
         std::memset(&f, 0, sizeof(f));
         f.sets = t.sets;
         f.set_of = t.set_of;
+        f.general = c->general;
         f.pos = t.pos;
         f.tri = d_tri;
         f.nn = d_nn;
@@ -686,7 +772,40 @@ int dgt_set_box(dgt_context *c, double Lx, double Ly)
     if (!c || c->batch || !(Lx > 0) || !(Ly > 0) || !std::isfinite(Lx) || !std::isfinite(Ly))
         return DGT_ERR_INVALID_ARGUMENT;
     c->boxes = { Lx, Ly };
+    c->general = 0;
     return init_context(c);
+}
+
+int dgt_set_box_general(dgt_context *c, double x11, double x12, double x21, double x22)
+{
+    if (!c || c->batch) return DGT_ERR_INVALID_ARGUMENT;
+    const double m[4] = { x11, x12, x21, x22 };
+    for (double v : m)
+        if (!std::isfinite(v)) return DGT_ERR_INVALID_ARGUMENT;
+    const double det = x11 * x22 - x12 * x21;
+    const double scale = (std::fabs(x11) + std::fabs(x21)) * (std::fabs(x12) + std::fabs(x22));
+    if (!(std::fabs(det) > 1e-12 * scale)) return DGT_ERR_INVALID_ARGUMENT;   // degenerate lattice
+    if (x12 == 0.0 && x21 == 0.0 && x11 > 0.0 && x22 > 0.0) return dgt_set_box(c, x11, x22);
+    double g[4] = { x11, x12, x21, x22 };
+    reduce_basis(g);
+    std::memcpy(c->gbox, g, sizeof(g));
+    c->general = 1;
+    c->boxes = { std::fabs(g[0]) + std::fabs(g[1]), std::fabs(g[2]) + std::fabs(g[3]) };
+    return init_context(c);
+}
+
+int dgt_get_box(const dgt_context *c, double *out4)
+{
+    if (!c || !out4 || c->batch) return DGT_ERR_INVALID_ARGUMENT;
+    if (c->general) {
+        std::memcpy(out4, c->gbox, sizeof(c->gbox));
+    } else {
+        out4[0] = c->boxes[0];
+        out4[1] = 0.0;
+        out4[2] = 0.0;
+        out4[3] = c->boxes[1];
+    }
+    return DGT_OK;
 }
 
 int dgt_set_safety_mode(dgt_context *c, int on)
@@ -888,7 +1007,8 @@ int dgt_validate(dgt_context *c, const double *d_points, const int *d_tri, const
     DGT_TRY(c->vcount.ensure(sizeof(unsigned long long) * 8));
     unsigned long long *d = c->vcount.as<unsigned long long>();
     DGT_TRY(launch_validate(c->d_sets.as<SetDesc>(), c->batch ? c->d_set_of.as<int>() : nullptr,
-                            reinterpret_cast<const double2 *>(d_points), d_tri, d_nn, stride, c->n, d, c->sms, s));
+                            reinterpret_cast<const double2 *>(d_points), d_tri, d_nn, stride, c->n, d, c->sms,
+                            c->general, s));
     unsigned long long h[7];
     DGT_TRY(cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, s));
     DGT_TRY(cudaStreamSynchronize(s));
@@ -968,7 +1088,9 @@ int ilog2(long long v)
 // mean spacing of a single-set context (cell sizes are absolute there)
 double spacing_of(const dgt_context *c)
 {
-    return std::sqrt(c->boxes[0] * c->boxes[1] / std::max(c->n, 1));
+    const double area = c->general ? std::fabs(c->gbox[0] * c->gbox[3] - c->gbox[1] * c->gbox[2])
+                                   : c->boxes[0] * c->boxes[1];
+    return std::sqrt(area / std::max(c->n, 1));
 }
 
 void set_relative_cell(dgt_context *c, double rel)

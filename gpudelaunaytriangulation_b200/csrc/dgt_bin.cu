@@ -20,10 +20,19 @@ namespace dgt {
 
 __device__ __forceinline__ int cell_index(const SetDesc &S, double2 p)
 {
-    int cx = (int)floor(p.x * S.icw), cy = (int)floor(p.y * S.ich);
+    const double2 f = S.general ? cell_pos<true>(S, p) : cell_pos<false>(S, p);
+    int cx = (int)floor(f.x), cy = (int)floor(f.y);
     cx = min(max(cx, 0), S.xsize - 1);
     cy = min(max(cy, 0), S.ysize - 1);
     return S.cell_base + cy * S.xsize + cx;
+}
+
+// Inputs the kernels accept: inside the rectangular box; any finite position for a general
+// box (its fractional coordinates are wrapped)
+__device__ __forceinline__ bool bad_input(const SetDesc &S, double2 p)
+{
+    if (S.general) return !(isfinite(p.x) && isfinite(p.y));
+    return !(p.x >= 0.0 && p.x < S.Lx && p.y >= 0.0 && p.y < S.Ly);
 }
 
 __device__ __forceinline__ bool skip(const int *cond) { return cond && *cond == 0; }
@@ -46,7 +55,7 @@ __global__ void __launch_bounds__(256) k_count(BinArgs a, DevStatus *st)
     if (i >= a.n) return;
     const SetDesc &S = a.sets[a.set_of ? a.set_of[i] : 0];
     double2 p = a.pos[i];
-    if (!(p.x >= 0.0 && p.x < S.Lx && p.y >= 0.0 && p.y < S.Ly)) {
+    if (bad_input(S, p)) {
         atomicOr(&st->err_flags, EF_BAD_INPUT);
         p = make_double2(0.0, 0.0);
     }
@@ -192,12 +201,12 @@ __global__ void __launch_bounds__(256) k_refresh(BinArgs a, DevStatus *st)
     if (i < a.n) {
         const SetDesc &S = a.sets[a.set_of ? a.set_of[i] : 0];
         double2 p = a.pos[i];
-        if (!(p.x >= 0.0 && p.x < S.Lx && p.y >= 0.0 && p.y < S.Ly)) {
+        if (bad_input(S, p)) {
             atomicOr(&st->err_flags, EF_BAD_INPUT);
             p = make_double2(0.0, 0.0);
         }
         a.spos[a.slot_of[i]] = p;
-        mv = outside_cell(S, a.cell_of[i], p);
+        mv = S.general ? outside_cell<true>(S, a.cell_of[i], p) : outside_cell<false>(S, a.cell_of[i], p);
     }
     for (int o = 16; o > 0; o >>= 1) mv = fmaxf(mv, __shfl_down_sync(0xffffffffu, mv, o));
     if ((threadIdx.x & 31) == 0 && mv > 0.0f) atomicMax(reinterpret_cast<int *>(&st->skin_measured), __float_as_int(mv));
@@ -298,8 +307,21 @@ __global__ void __launch_bounds__(256) k_displace(double2 *pos, int n, const Set
     double sn, cs;
     sincospi(2.0 * u2, &sn, &cs);
     double2 p = pos[i];
-    p.x = wrap_coord(p.x + r * cs, S.Lx);
-    p.y = wrap_coord(p.y + r * sn, S.Ly);
+    if (S.general) {
+        // periodicBoundaries::move (periodicBoundaries.h:181-189): displace, then back into
+        // the unit cell through fractional coordinates
+        p.x += r * cs;
+        p.y += r * sn;
+        double u = S.i11 * p.x + S.i12 * p.y, v = S.i21 * p.x + S.i22 * p.y;
+        u -= floor(u);
+        v -= floor(v);
+        if (!(u < 1.0)) u = 0.0;
+        if (!(v < 1.0)) v = 0.0;
+        p = make_double2(S.m11 * u + S.m12 * v, S.m21 * u + S.m22 * v);
+    } else {
+        p.x = wrap_coord(p.x + r * cs, S.Lx);
+        p.y = wrap_coord(p.y + r * sn, S.Ly);
+    }
     pos[i] = p;
 }
 

@@ -38,10 +38,28 @@ __device__ __noinline__ int incircle_exact_call(double2 a, double2 b, double2 d)
     return incircle_exact(a.x, a.y, b.x, b.y, d.x, d.y);
 }
 
-// float32 offset of q relative to p (minimum image, rounded once in double, then to float)
+// double offset of q relative to p (minimum image, rounded once; GEN: general box)
+template <bool GEN>
+__device__ __forceinline__ double2 off64(double2 q, double2 p, const SetDesc &S)
+{
+    return GEN ? gen_off(q, p, S) : make_double2(wrap_off(q.x, p.x, S.Lx, S.hLx), wrap_off(q.y, p.y, S.Ly, S.hLy));
+}
+
+// float32 offset of q relative to p (the double offset rounded to float)
+template <bool GEN>
 __device__ __forceinline__ float2 off32(double2 q, double2 p, const SetDesc &S)
 {
-    return make_float2(__double2float_rn(wrap_off(q.x, p.x, S.Lx, S.hLx)), __double2float_rn(wrap_off(q.y, p.y, S.Ly, S.hLy)));
+    const double2 d = off64<GEN>(q, p, S);
+    return make_float2(__double2float_rn(d.x), __double2float_rn(d.y));
+}
+
+// an offset within a quarter of the box's half extent per axis (cell units for a general box)
+template <bool GEN>
+__device__ __forceinline__ bool near_owner(double2 o, const SetDesc &S)
+{
+    if (GEN)
+        return fabs(S.g11 * o.x + S.g12 * o.y) < 0.25 * S.hxs && fabs(S.g21 * o.x + S.g22 * o.y) < 0.25 * S.hys;
+    return fabs(o.x) < 0.25 * S.hLx && fabs(o.y) < 0.25 * S.hLy;
 }
 
 // exact sign of "d strictly inside the circle through (0, a, b)" (CCW (0, a, b))
@@ -112,6 +130,7 @@ __device__ __forceinline__ unsigned long long claim_key(unsigned stamp, int slot
     return ((unsigned long long)stamp << 32) | x;
 }
 
+template <bool GEN>
 __global__ void __launch_bounds__(256, 2) k_flip_claim(FlipArgs A, int round)
 {
     const int ebase = *A.epoch_ptr + 1;
@@ -145,15 +164,11 @@ __global__ void __launch_bounds__(256, 2) k_flip_claim(FlipArgs A, int round)
                 row_load(A.tri + (size_t)a * A.stride, A.stride, ra);
                 row_load(A.tri + (size_t)b * A.stride, A.stride, rb);
                 const SetDesc S = A.sets[A.set_of ? A.set_of[i] : 0];
-                const double2 oa = make_double2(wrap_off(qa.x, p.x, S.Lx, S.hLx), wrap_off(qa.y, p.y, S.Ly, S.hLy));
-                const double2 oj = make_double2(wrap_off(qj.x, p.x, S.Lx, S.hLx), wrap_off(qj.y, p.y, S.Ly, S.hLy));
-                const double2 ob = make_double2(wrap_off(qb.x, p.x, S.Lx, S.hLx), wrap_off(qb.y, p.y, S.Ly, S.hLy));
+                const double2 oa = off64<GEN>(qa, p, S), oj = off64<GEN>(qj, p, S), ob = off64<GEN>(qb, p, S);
                 if (free_ab && incircle_staged(oa, oj, ob) > 0) {
                     // an illegal edge: flip it if the quadrilateral is consistent in all four
                     // rings, near the owning point and within the register rings, else rebuild
-                    const double qx = 0.25 * S.hLx, qy = 0.25 * S.hLy;
-                    bool ok = fabs(oa.x) < qx && fabs(oa.y) < qy && fabs(oj.x) < qx && fabs(oj.y) < qy &&
-                              fabs(ob.x) < qx && fabs(ob.y) < qy;
+                    bool ok = near_owner<GEN>(oa, S) && near_owner<GEN>(oj, S) && near_owner<GEN>(ob, S);
                     ok = ok && orient_staged(oa, ob) > 0 && mi > 3 && mj > 3;
                     ok = ok && ma >= 3 && mb >= 3 && ma < min(A.stride, RR) && mb < min(A.stride, RR);
                     int pr, sc;
@@ -180,6 +195,7 @@ __global__ void __launch_bounds__(256, 2) k_flip_claim(FlipArgs A, int round)
     }
 }
 
+template <bool GEN>
 __global__ void __launch_bounds__(256, 2) k_flip_apply(FlipArgs A, int round)
 {
     const int ebase = *A.epoch_ptr + 1;
@@ -235,8 +251,10 @@ __global__ void __launch_bounds__(256, 2) k_flip_apply(FlipArgs A, int round)
                 const double2 pi = __ldg(&A.pos[i]), pj = __ldg(&A.pos[j]), pa = __ldg(&A.pos[a]),
                               pb = __ldg(&A.pos[b]), px = __ldg(&A.pos[x]), py = __ldg(&A.pos[y]),
                               pz = __ldg(&A.pos[z]), pw = __ldg(&A.pos[w]);
-                const float2 ia = off32(pa, pi, S), ib = off32(pb, pi, S), ix = off32(px, pi, S), iy = off32(py, pi, S);
-                const float2 ja = off32(pa, pj, S), jb = off32(pb, pj, S), jz = off32(pz, pj, S), jw = off32(pw, pj, S);
+                const float2 ia = off32<GEN>(pa, pi, S), ib = off32<GEN>(pb, pi, S), ix = off32<GEN>(px, pi, S),
+                             iy = off32<GEN>(py, pi, S);
+                const float2 ja = off32<GEN>(pa, pj, S), jb = off32<GEN>(pb, pj, S), jz = off32<GEN>(pz, pj, S),
+                             jw = off32<GEN>(pw, pj, S);
                 if (incircle32(ix.x, ix.y, ia.x, ia.y, ib.x, ib.y) >= 0) out[k++] = make_int2(min(i, a), max(i, a));
                 if (incircle32(ia.x, ia.y, ib.x, ib.y, iy.x, iy.y) >= 0) out[k++] = make_int2(min(i, b), max(i, b));
                 if (incircle32(jb.x, jb.y, ja.x, ja.y, jz.x, jz.y) >= 0) out[k++] = make_int2(min(j, a), max(j, a));
@@ -276,10 +294,12 @@ int flip_grid(int sms) { return (sms > 0 ? sms : 148) * 8; }
 
 cudaError_t launch_flip_round(const FlipArgs &a, int round, int sms, cudaStream_t s)
 {
-    k_flip_claim<<<flip_grid(sms), 256, 0, s>>>(a, round);
+    if (a.general) k_flip_claim<true><<<flip_grid(sms), 256, 0, s>>>(a, round);
+    else k_flip_claim<false><<<flip_grid(sms), 256, 0, s>>>(a, round);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    k_flip_apply<<<flip_grid(sms), 256, 0, s>>>(a, round);
+    if (a.general) k_flip_apply<true><<<flip_grid(sms), 256, 0, s>>>(a, round);
+    else k_flip_apply<false><<<flip_grid(sms), 256, 0, s>>>(a, round);
     return cudaGetLastError();
 }
 

@@ -30,6 +30,17 @@ struct SetDesc {
     int bxsize;         // occupancy blocks per row (BLOCK_CELLS x BLOCK_CELLS cells each)
     int bysize;
     int block_base;     // first block of the set in the block-count array
+    // General periodic box (periodicBoundaries::setGeneral, periodicBoundaries.h:86-101): a
+    // point is M u with u its fractional coordinates, and the cell grid is a grid over u, so
+    // a cell is a parallelogram.  Used by the kernels' general-box instantiations only; the
+    // rectangular ones read the fields above (Lx, Ly, icw, ... then describe the box's
+    // bounding rectangle and are not used for geometry).
+    int general;
+    double m11, m12, m21, m22;   // box matrix; its columns are the two lattice vectors
+    double i11, i12, i21, i22;   // its inverse
+    double g11, g12, g21, g22;   // cells per unit of real offset: diag(xsize, ysize) * inverse
+    double gnx, gny;             // cells spanned per axis by a disc of unit radius (row norms of g)
+    double hxs, hys;             // half the grid, in cells: the reach of minimum-image offsets
 };
 
 constexpr int BLOCK_SHIFT = 3;   // occupancy blocks of 8 x 8 cells
@@ -52,13 +63,51 @@ __device__ __forceinline__ double arc_gap(double u, int c, int size)
     return u < lo ? fmin(lo - u, u + size - hi) : fmin(u - hi, lo + size - u);
 }
 
+// Position of p in cell units of its set's grid: [0, xsize) x [0, ysize) for a point inside
+// the box.  General box: the fractional coordinates are wrapped into [0, 1) first, so any
+// finite position is accepted (the result may equal xsize / ysize after rounding; cell
+// indices are clamped).
+template <bool GEN>
+__device__ __forceinline__ double2 cell_pos(const SetDesc &S, double2 p)
+{
+    if (!GEN) return make_double2(p.x * S.icw, p.y * S.ich);
+    double u = __fma_rn(S.i11, p.x, __dmul_rn(S.i12, p.y));
+    double v = __fma_rn(S.i21, p.x, __dmul_rn(S.i22, p.y));
+    u -= floor(u);
+    v -= floor(v);
+    return make_double2(u * (double)S.xsize, v * (double)S.ysize);
+}
+
+// General box: offset c - p to the image of c whose fractional offset lies in [-1/2, 1/2]
+// per component (the general branch of periodicBoundaries::minDist, periodicBoundaries.h:
+// 165-178).  The lattice shift l is chosen in fractional coordinates and taken off c when it
+// is positive, added to p otherwise, per axis: with a diagonal box matrix this is the
+// rectangular offset (wrap_off) bit for bit, except where a difference lies within rounding
+// of exactly half the box.  Explicit roundings throughout; the oracle performs the same
+// operations.
+__device__ __forceinline__ double gen_off1(double c, double p, double l)
+{
+    return l >= 0.0 ? __dsub_rn(__dsub_rn(c, l), p) : __dsub_rn(c, __dadd_rn(p, l));
+}
+__device__ __forceinline__ double2 gen_off(double2 c, double2 p, const SetDesc &S)
+{
+    const double dx = __dsub_rn(c.x, p.x), dy = __dsub_rn(c.y, p.y);
+    const double su = rint(__fma_rn(S.i11, dx, __dmul_rn(S.i12, dy)));
+    const double sv = rint(__fma_rn(S.i21, dx, __dmul_rn(S.i22, dy)));
+    const double lx = __fma_rn(S.m11, su, __dmul_rn(S.m12, sv));
+    const double ly = __fma_rn(S.m21, su, __dmul_rn(S.m22, sv));
+    return make_double2(gen_off1(c.x, p.x, lx), gen_off1(c.y, p.y, ly));
+}
+
 // How far, in cells per axis, point p now lies outside the cell c that lists it (0 while
 // inside), rounded up: the margin by which certification must widen while the cell lists
 // are kept (a point strictly inside a circle is listed by a cell within that margin of it).
+template <bool GEN = false>
 __device__ __forceinline__ float outside_cell(const SetDesc &S, int c, double2 p)
 {
     const int lc = c - S.cell_base, cy = lc / S.xsize, cx = lc - cy * S.xsize;
-    const double g = fmax(arc_gap(p.x * S.icw, cx, S.xsize), arc_gap(p.y * S.ich, cy, S.ysize));
+    const double2 f = cell_pos<GEN>(S, p);
+    const double g = fmax(arc_gap(f.x, cx, S.xsize), arc_gap(f.y, cy, S.ysize));
     return g > 0.0 ? (float)g * 1.0001f + 1e-6f : 0.0f;
 }
 
@@ -174,6 +223,7 @@ struct RingArgs {
     const float *skin;
     int cand_by_index;   // 1: candidate and own positions from pos[] through the index (repair)
     int check;         // 1: count float32 decisions contradicted by float64
+    int general = 0;   // 1: general-box instantiations (SetDesc::general)
     DevStatus *st;
 };
 
@@ -199,6 +249,7 @@ struct TestArgs {
     // cells of the last binning (index order; null: not measured): how far the points now
     // lie outside the cells that list them, largest -> st->skin_measured (outside_cell)
     const int *rcell_of;
+    int general = 0;        // 1: general-box instantiation (SetDesc::general)
     DevStatus *st;
 };
 
@@ -222,6 +273,7 @@ struct FlipArgs {
     int2 *next;                 // candidates of the next round
     int *next_count;
     int cap;                    // capacity of cur / next / quad
+    int general = 0;            // 1: general-box instantiations (SetDesc::general)
     DevStatus *st;
 };
 
@@ -248,7 +300,8 @@ constexpr int DEFAULT_WORK_BUDGET = 4096;
 cudaError_t launch_test(const TestArgs &a, cudaStream_t s);
 // device validation counts (sum, bad_rows, asymmetric, not_ccw, winding, not_delaunay, points)
 cudaError_t launch_validate(const SetDesc *sets, const int *set_of, const double2 *pos, const int *tri,
-                            const int *nn, int stride, int n, unsigned long long *out, int sms, cudaStream_t s);
+                            const int *nn, int stride, int n, unsigned long long *out, int sms, int general,
+                            cudaStream_t s);
 cudaError_t launch_flip_round(const FlipArgs &a, int round, int sms, cudaStream_t s);
 // leftover candidates to the rebuild list; advances the context's flip stamp by rounds + 1
 cudaError_t launch_flip_spill(const FlipArgs &a, int rounds, DevCtl *ctl, int sms, cudaStream_t s);

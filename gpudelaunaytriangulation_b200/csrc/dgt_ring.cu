@@ -144,12 +144,46 @@ __device__ __noinline__ double4 circle64(const double2 *pos, double2 p, double L
     return make_circ<double>(a.x, a.y, b.x, b.y);
 }
 
+// the same three for a general box (S: the set's descriptor in global memory)
+__device__ __forceinline__ double2 off64g(const double2 *pos, double2 p, const SetDesc *S, int id)
+{
+    if (id >= 0) return gen_off(__ldg(&pos[id]), p, *S);
+    int c = -id - 1;
+    double v = (double)S->V;
+    return make_double2((c == 0 || c == 3) ? v : -v, (c < 2) ? v : -v);
+}
+template <bool EXACT>
+__device__ __noinline__ int recheck64g(const double2 *pos, double2 p, const SetDesc *S, int ia, int ib, double dx,
+                                       double dy)
+{
+    double2 a = off64g(pos, p, S, ia), b = off64g(pos, p, S, ib);
+    int r = incircle64(a.x, a.y, b.x, b.y, dx, dy);
+    if (r != 0 || !EXACT) return r;
+    r = incircle_exact(a.x, a.y, b.x, b.y, dx, dy);
+    return r > 0 ? 2 : -2;
+}
+__device__ __noinline__ int check64g(const double2 *pos, double2 p, const SetDesc *S, int ia, int ib, double dx,
+                                     double dy, int inside)
+{
+    double2 a = off64g(pos, p, S, ia), b = off64g(pos, p, S, ib);
+    int r = incircle64(a.x, a.y, b.x, b.y, dx, dy);
+    return (inside && r < 0) || (!inside && r > 0) ? 1 : 0;
+}
+__device__ __noinline__ double4 circle64g(const double2 *pos, double2 p, const SetDesc *S, int ia, int ib)
+{
+    double2 a = off64g(pos, p, S, ia), b = off64g(pos, p, S, ib);
+    return make_circ<double>(a.x, a.y, b.x, b.y);
+}
+
 // ------------------------------------------------------------------- the construction
 // CAND: where candidate positions come from -- 0 the cell-order copy (current after a
 // binning), 1 the caller's positions through the index (repair: the cell lists may be older
-// than the positions), 2 chosen at run time by A.cand_by_index
-template <typename T, bool EXACT, class Ring, class C = Ctr, int CAND = 2>
+// than the positions), 2 chosen at run time by A.cand_by_index.  GEN: general periodic box
+// (offsets, cells and certification in the box's fractional frame; Sg: the set's descriptor
+// in global memory, for the out-of-line float64 paths)
+template <typename T, bool EXACT, class Ring, class C = Ctr, int CAND = 2, bool GEN = false>
 struct Builder {
+    static constexpr bool general = GEN;
     typedef Prec<T> PR;
     typedef typename PR::T4 E4;
     typedef typename PR::T2 V2;
@@ -157,6 +191,7 @@ struct Builder {
 
     const RingArgs &A;
     const SetDesc &S;
+    const SetDesc *Sg;
     Ring &R;
     C &ctr;
     double2 p;
@@ -166,8 +201,9 @@ struct Builder {
     int ocx, ocy;
     bool minimage = false;   // the certified circles reach past half the box
 
-    __device__ Builder(const RingArgs &a, const SetDesc &s, Ring &r, C &c, double2 pp, int sl)
-        : A(a), S(s), R(r), ctr(c), p(pp), slot(sl), m(0), r2max((T)0), ocx(0), ocy(0) {}
+    __device__ Builder(const RingArgs &a, const SetDesc &s, Ring &r, C &c, double2 pp, int sl,
+                       const SetDesc *sg = nullptr)
+        : A(a), S(s), Sg(sg), R(r), ctr(c), p(pp), slot(sl), m(0), r2max((T)0), ocx(0), ocy(0) {}
 
     // r2max bounds |d|^2 for any d inside some edge circle (a circle through the origin of
     // radius <= rc lies within 2 rc of it): the candidate prefilter.  Exact maximum here;
@@ -200,7 +236,8 @@ struct Builder {
         if (!EXACT) R.work() = 0;
         m = 4;
         refresh_r2max();
-        int cx = (int)floor(p.x * S.icw), cy = (int)floor(p.y * S.ich);
+        const double2 f = cell_pos<GEN>(S, p);
+        int cx = (int)floor(f.x), cy = (int)floor(f.y);
         ocx = min(max(cx, 0), S.xsize - 1);
         ocy = min(max(cy, 0), S.ysize - 1);
     }
@@ -215,7 +252,8 @@ struct Builder {
     __device__ __forceinline__ int recheck(int k, double2 d64)
     {
         int ia = R.idx(k), ib = R.idx(k + 1 == m ? 0 : k + 1);
-        int r = recheck64<EXACT>(A.pos, p, S.Lx, S.hLx, S.Ly, S.hLy, S.V, ia, ib, d64.x, d64.y);
+        int r = GEN ? recheck64g<EXACT>(A.pos, p, Sg, ia, ib, d64.x, d64.y)
+                    : recheck64<EXACT>(A.pos, p, S.Lx, S.hLx, S.Ly, S.hLy, S.V, ia, ib, d64.x, d64.y);
         if (r == 2 || r == -2 || r == 0) ctr.add_u64();
         return r > 0 ? 1 : (r < 0 ? -1 : 0);
     }
@@ -268,7 +306,8 @@ struct Builder {
         // than the positions (cell lists kept from the last binning)
         const bool by_index = CAND == 1 || (CAND == 2 && A.cand_by_index);
         double2 q = by_index ? __ldg(&A.pos[__ldg(&A.sidx[sl])]) : __ldg(&A.spos[sl]);
-        double2 d64 = make_double2(wrap_off(q.x, p.x, S.Lx, S.hLx), wrap_off(q.y, p.y, S.Ly, S.hLy));
+        double2 d64 = GEN ? gen_off(q, p, S)
+                          : make_double2(wrap_off(q.x, p.x, S.Lx, S.hLx), wrap_off(q.y, p.y, S.Ly, S.hLy));
         if (d64.x == 0.0 && d64.y == 0.0) return R_OK;   // coincident point
         ctr.cand++;
         d = PR::mk2(PR::from64(d64.x), PR::from64(d64.y));
@@ -300,8 +339,9 @@ struct Builder {
             for (int k = 0; k < m; ++k) {
                 if ((open >> k) & 1) continue;
                 int ia = R.idx(k), ib = R.idx(k + 1 == m ? 0 : k + 1);
-                ctr.add_mism(check64(A.pos, p, S.Lx, S.hLx, S.Ly, S.hLy, S.V, ia, ib, d64.x, d64.y,
-                                    (int)((mask >> k) & 1)));
+                ctr.add_mism(GEN ? check64g(A.pos, p, Sg, ia, ib, d64.x, d64.y, (int)((mask >> k) & 1))
+                                 : check64(A.pos, p, S.Lx, S.hLx, S.Ly, S.hLy, S.V, ia, ib, d64.x, d64.y,
+                                           (int)((mask >> k) & 1)));
             }
         }
         return R_OK;
@@ -385,6 +425,7 @@ struct Builder {
     // bounding boxes.  Returns false when some circle cannot be bounded (whole box needed).
     __device__ bool need_rect(double fx, double fy, int &lx, int &hx, int &ly, int &hy)
     {
+        if (GEN) return need_rect_gen(fx, fy, lx, hx, ly, hy);
         double xmin = 1e300, xmax = -1e300, ymin = 1e300, ymax = -1e300;
         T mx = (T)0;
         bool finite = true;
@@ -432,6 +473,57 @@ struct Builder {
         return true;
     }
 
+    // General box: the same in cell units.  A circle (c, rc) maps to an ellipse in cell
+    // coordinates, centred at g c, whose bounding box spans rc times the row norms of g.
+    __device__ bool need_rect_gen(double fx, double fy, int &lx, int &hx, int &ly, int &hy)
+    {
+        double umin = 1e300, umax = -1e300, vmin = 1e300, vmax = -1e300;
+        T mx = (T)0;
+        bool finite = true;
+        for (int k = 0; k < m; ++k) {
+            E4 e = R.edge(k);
+            double cx, cy, rc;
+            mx = e.w > mx ? e.w : mx;
+            finite &= e.w < PR::inf();
+            if (e.w < PR::inf()) {
+                cx = 0.5 * (double)e.x;
+                cy = 0.5 * (double)e.y;
+                rc = (double)e.w;
+            } else {
+                int ia = R.idx(k), ib = R.idx(k + 1 == m ? 0 : k + 1);
+                double4 c = circle64g(A.pos, p, Sg, ia, ib);
+                if (!(c.w < Prec<double>::inf())) {
+                    minimage = true;
+                    return false;
+                }
+                cx = 0.5 * c.x;
+                cy = 0.5 * c.y;
+                rc = c.w;
+            }
+            const double uc = S.g11 * cx + S.g12 * cy, vc = S.g21 * cx + S.g22 * cy;
+            const double hu = rc * S.gnx, hv = rc * S.gny;
+            umin = fmin(umin, uc - hu);
+            umax = fmax(umax, uc + hu);
+            vmin = fmin(vmin, vc - hv);
+            vmax = fmax(vmax, vc + hv);
+        }
+        if (finite) r2max = r2_of(mx);
+        // fractional offsets are unique within half the box per axis (hxs, hys cells)
+        minimage = umin < -S.hxs || umax > S.hxs || vmin < -S.hys || vmax > S.hys;
+        const double sk = A.skin ? (double)*A.skin : 0.0;
+        double a0 = fx + umin - sk, a1 = fx + umax + sk;
+        double b0 = fy + vmin - sk, b1 = fy + vmax + sk;
+        a0 -= 1e-9 * (1.0 + fabs(a0));
+        a1 += 1e-9 * (1.0 + fabs(a1));
+        b0 -= 1e-9 * (1.0 + fabs(b0));
+        b1 += 1e-9 * (1.0 + fabs(b1));
+        lx = (int)fmax(floor(a0), -1e8);
+        hx = (int)fmin(floor(a1), 1e8);
+        ly = (int)fmax(floor(b0), -1e8);
+        hy = (int)fmin(floor(b1), 1e8);
+        return true;
+    }
+
     // Whether the cell (rx, ry) (relative to the own cell) may hold a point strictly inside
     // some edge circle: its rectangle, widened by a margin far above the rounding of cell
     // indices and offsets, meets a disc (c~, rc) that contains the exact circle.  Cells
@@ -446,6 +538,7 @@ struct Builder {
     // the same for the cells [rx0, rx1] x [ry0, ry1] together
     __device__ bool rect_reached(int rx0, int rx1, int ry0, int ry1, double fx, double fy)
     {
+        if (GEN) return rect_reached_gen(rx0, rx1, ry0, ry1, fx, fy);
         const double mg = 1e-9;
         const double sk = A.skin ? (double)*A.skin : 0.0;   // see need_rect
         double a0 = (double)rx0 - fx - sk, a1 = (double)rx1 - fx + 1.0 + sk;
@@ -464,13 +557,37 @@ struct Builder {
         }
         return false;
     }
+    // general box: the cells against each circle's ellipse bounding box in cell units (a
+    // superset of the ellipse, so a cell judged unreached is unreached)
+    __device__ bool rect_reached_gen(int rx0, int rx1, int ry0, int ry1, double fx, double fy)
+    {
+        const double mg = 1e-9;
+        const double sk = A.skin ? (double)*A.skin : 0.0;
+        double a0 = (double)rx0 - fx - sk, a1 = (double)rx1 - fx + 1.0 + sk;
+        double b0 = (double)ry0 - fy - sk, b1 = (double)ry1 - fy + 1.0 + sk;
+        a0 -= mg * (1.0 + fabs(a0));
+        a1 += mg * (1.0 + fabs(a1));
+        b0 -= mg * (1.0 + fabs(b0));
+        b1 += mg * (1.0 + fabs(b1));
+        if (a0 < -S.hxs || a1 > S.hxs || b0 < -S.hys || b1 > S.hys) return true;
+        for (int k = 0; k < m; ++k) {
+            E4 e = R.edge(k);
+            if (!(e.w < PR::inf())) return true;
+            const double cx = 0.5 * (double)e.x, cy = 0.5 * (double)e.y, rc = (double)e.w * (1.0 + mg);
+            const double uc = S.g11 * cx + S.g12 * cy, vc = S.g21 * cx + S.g22 * cy;
+            const double hu = rc * S.gnx, hv = rc * S.gny;
+            if (uc + hu >= a0 && uc - hu <= a1 && vc + hv >= b0 && vc - hv <= b1) return true;
+        }
+        return false;
+    }
 
     // Called by every lane of the warp (warp votes inside); `active` false for lanes
     // without a point.  Returns R_OK / error for active lanes.
     __device__ int run(bool active)
     {
         init();
-        const double fx = p.x * S.icw - (double)ocx, fy = p.y * S.ich - (double)ocy;
+        const double2 fp = cell_pos<GEN>(S, p);
+        const double fx = fp.x - (double)ocx, fy = fp.y - (double)ocy;
         int x0 = 0, x1 = 0, y0 = 0, y1 = 0;
         const int max_phase = S.xsize + S.ysize + 8;
         bool done = !active;
@@ -661,8 +778,9 @@ __device__ __forceinline__ int item_count(const RingArgs &A)
 }
 
 // hot kernel: shared-memory ring of CAP entries per thread; IDX: candidate and own positions
-// through the index (repair rounds), else from the cell-order copy (global build)
-template <typename T, int CAP, int BLOCK, bool IDX>
+// through the index (repair rounds), else from the cell-order copy (global build); GEN:
+// general periodic box
+template <typename T, int CAP, int BLOCK, bool IDX, bool GEN = false>
 __global__ void __launch_bounds__(BLOCK) k_build(RingArgs A)
 {
     typedef typename Prec<T>::T4 E4;
@@ -697,9 +815,11 @@ __global__ void __launch_bounds__(BLOCK) k_build(RingArgs A)
                 pid = __ldg(&A.sidx[t]);
             }
         }
-        const SetDesc S = A.sets[(act && A.set_of) ? __ldg(&A.set_of[slot]) : 0];
+        const int si = (act && A.set_of) ? __ldg(&A.set_of[slot]) : 0;
+        const SetDesc S = A.sets[si];
         double2 p = !act ? make_double2(0.0, 0.0) : (IDX ? __ldg(&A.pos[pid]) : __ldg(&A.spos[slot]));
-        Builder<T, false, SmemRing<T, CAP, BLOCK>, SmemCtr<BLOCK>, IDX ? 1 : 0> b(A, S, ring, ctr, p, slot);
+        Builder<T, false, SmemRing<T, CAP, BLOCK>, SmemCtr<BLOCK>, IDX ? 1 : 0, GEN> b(A, S, ring, ctr, p, slot,
+                                                                                    A.sets + si);
         int r = b.run(act);
         if (act) {
             pts++;
@@ -760,7 +880,8 @@ __device__ int coop_run(B &b, const int lane)
     if (lane == 0) b.init_ring();
     __syncwarp();
     b.init_local();
-    const double fx = b.p.x * S.icw - (double)b.ocx, fy = b.p.y * S.ich - (double)b.ocy;
+    const double2 fp = cell_pos<B::general>(S, b.p);
+    const double fx = fp.x - (double)b.ocx, fy = fp.y - (double)b.ocy;
     int x0 = 0, x1 = 0, y0 = 0, y1 = 0;
     bool changed = true;
     int status = R_OK;
@@ -925,6 +1046,7 @@ __device__ int coop_run(B &b, const int lane)
     return R_OK;
 }
 
+template <bool GEN>
 __global__ void __launch_bounds__(WARP_KERNEL_WARPS * 32, 4) k_build_warp(RingArgs A)
 {
     __shared__ float4 se[WARP_KERNEL_CAP][WARP_KERNEL_WARPS];
@@ -949,9 +1071,11 @@ __global__ void __launch_bounds__(WARP_KERNEL_WARPS * 32, 4) k_build_warp(RingAr
         const int pid = e < 0 ? ~e : e;
         heavy += e < 0;
         const int slot = A.slot_of[pid];
-        const SetDesc S = A.sets[A.set_of ? A.set_of[slot] : 0];
+        const int si = A.set_of ? A.set_of[slot] : 0;
+        const SetDesc S = A.sets[si];
         const double2 p = A.cand_by_index ? A.pos[pid] : A.spos[slot];
-        Builder<float, true, SmemRing<float, WARP_KERNEL_CAP, WARP_KERNEL_WARPS>> b(A, S, ring, ctr, p, slot);
+        Builder<float, true, SmemRing<float, WARP_KERNEL_CAP, WARP_KERNEL_WARPS>, Ctr, 2, GEN> b(A, S, ring, ctr, p,
+                                                                                              slot, A.sets + si);
         const int r = coop_run(b, lane);
         if (lane == 0) {
             pts++;
@@ -1044,6 +1168,7 @@ __device__ __forceinline__ void test_spoke(double2 prev, double2 cur, double2 nx
 // Flip mode (A.flip_list set): a valid fan (every triangle strictly CCW, winding once) sends
 // its illegal or undecided spokes (i, P_k) with i < P_k to the flip list (the flip stage
 // decides them exactly); an invalid fan queues its point for rebuilding.
+template <bool GEN>
 __global__ void __launch_bounds__(256) k_test(TestArgs A)
 {
     unsigned long long flagged = 0;
@@ -1065,8 +1190,10 @@ __global__ void __launch_bounds__(256) k_test(TestArgs A)
         if (t < A.n && A.rcell_of) {
             const SetDesc S = A.sets[A.set_of ? A.set_of[i] : 0];
             const double2 p = A.pos[i];
-            if (!(p.x >= 0.0 && p.x < S.Lx && p.y >= 0.0 && p.y < S.Ly)) atomicOr(&A.st->err_flags, EF_BAD_INPUT);
-            moved = fmaxf(moved, outside_cell(S, A.rcell_of[i], p));
+            const bool bad_in = GEN ? !(isfinite(p.x) && isfinite(p.y))
+                                    : !(p.x >= 0.0 && p.x < S.Lx && p.y >= 0.0 && p.y < S.Ly);
+            if (bad_in) atomicOr(&A.st->err_flags, EF_BAD_INPUT);
+            moved = fmaxf(moved, outside_cell<GEN>(S, A.rcell_of[i], p));
         }
         if (t < A.n) {
             int m = A.nn[i];
@@ -1083,8 +1210,10 @@ __global__ void __launch_bounds__(256) k_test(TestArgs A)
                 const SetDesc S = A.sets[A.set_of ? A.set_of[i] : 0];
                 double2 p = (A.sidx && !flip) ? A.spos[t] : A.pos[i];
                 double2 q0 = __ldg(&A.pos[row[0]]), ql = __ldg(&A.pos[row[m - 1]]);
-                double2 o0 = make_double2(wrap_off(q0.x, p.x, S.Lx, S.hLx), wrap_off(q0.y, p.y, S.Ly, S.hLy));
-                double2 prev = make_double2(wrap_off(ql.x, p.x, S.Lx, S.hLx), wrap_off(ql.y, p.y, S.Ly, S.hLy));
+                double2 o0 = GEN ? gen_off(q0, p, S)
+                                 : make_double2(wrap_off(q0.x, p.x, S.Lx, S.hLx), wrap_off(q0.y, p.y, S.Ly, S.hLy));
+                double2 prev = GEN ? gen_off(ql, p, S)
+                                   : make_double2(wrap_off(ql.x, p.x, S.Lx, S.hLx), wrap_off(ql.y, p.y, S.Ly, S.hLy));
                 double2 cur = o0;
                 int cross = 0;
                 // neighbour positions gathered two spokes ahead of their use
@@ -1095,7 +1224,8 @@ __global__ void __launch_bounds__(256) k_test(TestArgs A)
                     if (k + 3 < m) qb = __ldg(&A.pos[row[k + 3]]);
                     double2 nxt;
                     if (k + 1 < m) {
-                        nxt = make_double2(wrap_off(qn.x, p.x, S.Lx, S.hLx), wrap_off(qn.y, p.y, S.Ly, S.hLy));
+                        nxt = GEN ? gen_off(qn, p, S)
+                                  : make_double2(wrap_off(qn.x, p.x, S.Lx, S.hLx), wrap_off(qn.y, p.y, S.Ly, S.hLy));
                     } else {
                         nxt = o0;
                     }
@@ -1151,7 +1281,7 @@ __global__ void __launch_bounds__(256) k_test(TestArgs A)
 }
 
 // ------------------------------------------------------------------------- launchers
-template <typename T, int CAP, int BLOCK>
+template <typename T, int CAP, int BLOCK, bool GEN = false>
 static cudaError_t launch_build_t(const RingArgs &a, int sms, cudaStream_t s)
 {
     int blocks;
@@ -1162,8 +1292,8 @@ static cudaError_t launch_build_t(const RingArgs &a, int sms, cudaStream_t s)
         blocks = (a.n_items + BLOCK - 1) / BLOCK;
     }
     if (blocks < 1) blocks = 1;
-    if (a.cand_by_index) k_build<T, CAP, BLOCK, true><<<blocks, BLOCK, 0, s>>>(a);
-    else k_build<T, CAP, BLOCK, false><<<blocks, BLOCK, 0, s>>>(a);
+    if (a.cand_by_index) k_build<T, CAP, BLOCK, true, GEN><<<blocks, BLOCK, 0, s>>>(a);
+    else k_build<T, CAP, BLOCK, false, GEN><<<blocks, BLOCK, 0, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -1178,6 +1308,11 @@ int kernel_shape_block(int shape) { return (shape >= 0 && shape < KERNEL_SHAPES)
 cudaError_t launch_build(const RingArgs &a, int mode, int sms, int shape, cudaStream_t s)
 {
     if (a.n_items <= 0) return cudaSuccess;
+    if (a.general) {
+        // general boxes: the default shape only (rings past its capacity go to the warp kernel)
+        if (mode == MODE_F64) return launch_build_t<double, 14, 64, true>(a, sms, s);
+        return launch_build_t<float, 14, 64, true>(a, sms, s);
+    }
     if (mode == MODE_F64) return launch_build_t<double, 14, 64>(a, sms, s);
     switch (shape) {
     case 1: return launch_build_t<float, 12, 64>(a, sms, s);
@@ -1190,7 +1325,8 @@ cudaError_t launch_build(const RingArgs &a, int mode, int sms, int shape, cudaSt
 
 cudaError_t launch_deferred(const RingArgs &a, int sms, cudaStream_t s)
 {
-    k_build_warp<<<max(sms, 1) * 4, WARP_KERNEL_WARPS * 32, 0, s>>>(a);
+    if (a.general) k_build_warp<true><<<max(sms, 1) * 4, WARP_KERNEL_WARPS * 32, 0, s>>>(a);
+    else k_build_warp<false><<<max(sms, 1) * 4, WARP_KERNEL_WARPS * 32, 0, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -1198,7 +1334,8 @@ cudaError_t launch_test(const TestArgs &a, cudaStream_t s)
 {
     if (a.n <= 0) return cudaSuccess;
     int blocks = (a.n + 255) / 256;
-    k_test<<<blocks, 256, 0, s>>>(a);
+    if (a.general) k_test<true><<<blocks, 256, 0, s>>>(a);
+    else k_test<false><<<blocks, 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -51,6 +51,7 @@ struct ValidateArgs {
 
 constexpr int V_COUNTS = 7;
 
+template <bool GEN>
 __global__ void __launch_bounds__(256) k_validate(ValidateArgs A)
 {
     unsigned long long c[V_COUNTS] = { 0, 0, 0, 0, 0, 0, 0 };
@@ -75,7 +76,7 @@ __global__ void __launch_bounds__(256) k_validate(ValidateArgs A)
         const double2 p = A.pos[i];
         auto off = [&](int j) {
             const double2 q = A.pos[j];
-            return make_double2(wrap_off(q.x, p.x, S.Lx, S.hLx), wrap_off(q.y, p.y, S.Ly, S.hLy));
+            return GEN ? gen_off(q, p, S) : make_double2(wrap_off(q.x, p.x, S.Lx, S.hLx), wrap_off(q.y, p.y, S.Ly, S.hLy));
         };
         double2 prev = off(row[m - 1]), cur = off(row[0]);
         int cross = 0;
@@ -117,7 +118,8 @@ __global__ void __launch_bounds__(256) k_validate(ValidateArgs A)
 }  // namespace
 
 cudaError_t launch_validate(const SetDesc *sets, const int *set_of, const double2 *pos, const int *tri,
-                            const int *nn, int stride, int n, unsigned long long *out, int sms, cudaStream_t s)
+                            const int *nn, int stride, int n, unsigned long long *out, int sms, int general,
+                            cudaStream_t s)
 {
     ValidateArgs a{ sets, set_of, pos, tri, nn, stride, n, out };
     cudaError_t e = cudaMemsetAsync(out, 0, sizeof(unsigned long long) * V_COUNTS, s);
@@ -125,7 +127,8 @@ cudaError_t launch_validate(const SetDesc *sets, const int *set_of, const double
     int blocks = (n + 255) / 256;
     const int cap = (sms > 0 ? sms : 148) * 8;
     if (blocks > cap) blocks = cap;
-    k_validate<<<blocks, 256, 0, s>>>(a);
+    if (general) k_validate<true><<<blocks, 256, 0, s>>>(a);
+    else k_validate<false><<<blocks, 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 

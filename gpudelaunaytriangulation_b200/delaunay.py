@@ -26,15 +26,56 @@ from . import _native as _nat
 
 @dataclass
 class PeriodicBox:
-    """Rectangular periodic box [0, Lx) x [0, Ly) (periodicBoundaries(x, y),
-    src/utilities/periodicBoundaries.h:30)."""
+    """Periodic box (src/utilities/periodicBoundaries.h).  PeriodicBox(Lx, Ly) is the
+    rectangle [0, Lx) x [0, Ly) (periodicBoundaries(x, y), :30); PeriodicBox(xx, yy, xy, yx),
+    or PeriodicBox.general(xx, xy, yx, yy) in the reference's argument order, is the general
+    box of periodicBoundaries(a, b, c, d) (:32, setGeneral :86-101): a point is
+    (xx u + xy v, yx u + yy v) for fractional coordinates (u, v)."""
 
     Lx: float
     Ly: float
+    xy: float = 0.0
+    yx: float = 0.0
+
+    @classmethod
+    def general(cls, xx: float, xy: float, yx: float, yy: float) -> "PeriodicBox":
+        return cls(float(xx), float(yy), float(xy), float(yx))
+
+    @classmethod
+    def of(cls, box) -> "PeriodicBox":
+        """A PeriodicBox, an (Lx, Ly) pair or a general (xx, xy, yx, yy) matrix."""
+        if isinstance(box, PeriodicBox):
+            return box
+        box = tuple(float(v) for v in box)
+        if len(box) == 2:
+            return cls(*box)
+        if len(box) == 4:
+            return cls.general(*box)
+        raise ValueError("a box is (Lx, Ly) or (xx, xy, yx, yy)")
+
+    def isBoxSquare(self) -> bool:
+        """periodicBoundaries::isBoxSquare (:39): rectangular."""
+        return self.xy == 0.0 and self.yx == 0.0
+
+    def getBoxDims(self):
+        """periodicBoundaries::getBoxDims (:36): (xx, xy, yx, yy)."""
+        return self.Lx, self.xy, self.yx, self.Ly
 
     def putInBoxReal(self, p: torch.Tensor) -> torch.Tensor:
         """Wrap points into the primary cell (periodicBoundaries.h:131-152)."""
         out = p.clone()
+        if not self.isBoxSquare():
+            xx, xy, yx, yy = self.getBoxDims()
+            det = xx * yy - xy * yx
+            u = (yy * out[..., 0] - xy * out[..., 1]) / det
+            v = (-yx * out[..., 0] + xx * out[..., 1]) / det
+            u = torch.remainder(u, 1.0)
+            v = torch.remainder(v, 1.0)
+            u = torch.where(u >= 1.0, torch.zeros_like(u), u)
+            v = torch.where(v >= 1.0, torch.zeros_like(v), v)
+            out[..., 0] = xx * u + xy * v
+            out[..., 1] = yx * u + yy * v
+            return out
         out[..., 0] = torch.remainder(out[..., 0], self.Lx)
         out[..., 1] = torch.remainder(out[..., 1], self.Ly)
         out[..., 0] = torch.where(out[..., 0] >= self.Lx, torch.zeros_like(out[..., 0]), out[..., 0])
@@ -82,12 +123,24 @@ class DelaunayGPU:
         else:
             if box is None:
                 raise ValueError("a periodic box is required")
-            if not isinstance(box, PeriodicBox):
-                box = PeriodicBox(float(box[0]), float(box[1]))
+            box = PeriodicBox.of(box)
             self.Box = box
             self.Ncells = int(N)
-            _nat.check(lib.dgt_create(self.Ncells, int(maximumNeighborsGuess), float(cellSize), box.Lx, box.Ly,
-                                     ctypes.byref(self._h)), "dgt_create")
+            if box.isBoxSquare():
+                _nat.check(lib.dgt_create(self.Ncells, int(maximumNeighborsGuess), float(cellSize), box.Lx, box.Ly,
+                                         ctypes.byref(self._h)), "dgt_create")
+            else:
+                # created on the bounding rectangle, then given the general box
+                bx = abs(box.Lx) + abs(box.xy)
+                by = abs(box.yx) + abs(box.Ly)
+                _nat.check(lib.dgt_create(self.Ncells, int(maximumNeighborsGuess), float(cellSize), bx, by,
+                                         ctypes.byref(self._h)), "dgt_create")
+                try:
+                    _nat.check(lib.dgt_set_box_general(self._h, *box.getBoxDims()), "dgt_set_box_general")
+                except Exception:
+                    lib.dgt_destroy(self._h)
+                    self._h = ctypes.c_void_p()
+                    raise
         self.safetyMode = True
         self.GPUcompute = True
         self.last_stats: dict | None = None
@@ -107,10 +160,20 @@ class DelaunayGPU:
         _nat.check(self._L.dgt_set_cell_size(self._h, float(csize)), "dgt_set_cell_size")
 
     def setBox(self, box: PeriodicBox | tuple):
-        if not isinstance(box, PeriodicBox):
-            box = PeriodicBox(float(box[0]), float(box[1]))
-        _nat.check(self._L.dgt_set_box(self._h, box.Lx, box.Ly), "dgt_set_box")
+        """setBox(bx) (DelaunayGPU.h:44): rectangular or general box."""
+        box = PeriodicBox.of(box)
+        if box.isBoxSquare():
+            _nat.check(self._L.dgt_set_box(self._h, box.Lx, box.Ly), "dgt_set_box")
+        else:
+            _nat.check(self._L.dgt_set_box_general(self._h, *box.getBoxDims()), "dgt_set_box_general")
         self.Box = box
+
+    def kernelBox(self):
+        """The box matrix (xx, xy, yx, yy) the kernels use: the reduced basis of a general box
+        (the same lattice), (Lx, 0, 0, Ly) for a rectangle."""
+        out = (ctypes.c_double * 4)()
+        _nat.check(self._L.dgt_get_box(self._h, out), "dgt_get_box")
+        return tuple(out)
 
     def setSafetyMode(self, flag: bool):
         self.safetyMode = bool(flag)

@@ -120,6 +120,19 @@ int dgt_update_list(dgt_context *ctx, const double *d_points, void *stream);
 int dgt_set_cell_size(dgt_context *ctx, double cell_size);
 /* setBox(bx) (DelaunayGPU.h:44); single-set contexts only */
 int dgt_set_box(dgt_context *ctx, double Lx, double Ly);
+/* setBox with a general (non-rectangular) periodicBoundaries box, setGeneral(a, b, c, d)
+ * (periodicBoundaries.h:86-101): a point is (x11 u + x12 v, x21 u + x22 v) for fractional
+ * coordinates (u, v), i.e. the lattice vectors are the columns (x11, x21) and (x12, x22).  The
+ * reference's cell list and kernels are rectangular-only (cellListGPU.h:14-16); here the
+ * kernels run in the box's fractional frame.  The basis is first reduced (Lagrange-Gauss: the
+ * same lattice, most nearly orthogonal basis; the triangulation depends on the lattice only).
+ * Points may lie anywhere (fractional coordinates are wrapped); non-finite coordinates raise
+ * DGT_EF_BAD_INPUT.  A diagonal matrix with positive entries is dgt_set_box.  Single-set
+ * contexts only; DGT_ERR_INVALID_ARGUMENT for a degenerate or non-finite matrix. */
+int dgt_set_box_general(dgt_context *ctx, double x11, double x12, double x21, double x22);
+/* getBoxDims(xx, xy, yx, yy) (periodicBoundaries.h:36-37) of the box the kernels use: the
+ * reduced basis after dgt_set_box_general, (Lx, 0, 0, Ly) for a rectangular box. */
+int dgt_get_box(const dgt_context *ctx, double *out4);
 /* setSafetyMode(sm) (DelaunayGPU.h:46).  On: each call synchronises and reports
  * DGT_ERR_NEED_RESIZE.  Off: calls return without synchronising; overflowing rings are
  * written with neighnum 0 and show in dgt_get_stats (never silently truncated). */

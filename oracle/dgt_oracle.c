@@ -474,6 +474,81 @@ void orc_offset(const double *c, const double *p, double Lx, double Ly, double *
     out[1] = dgt_offset1(c[1], p[1], Ly);
 }
 
+/* General periodic box (periodicBoundaries::setGeneral, src/utilities/periodicBoundaries.h:
+   86-101): a point is M u for fractional coordinates u, M = {{x11, x12}, {x21, x22}} (box[0..3]
+   = x11, x12, x21, x22).  The offset c - p goes to the image whose fractional offset lies in
+   [-1/2, 1/2] per component, as periodicBoundaries::minDist does for a general box
+   (:165-178): the integer lattice shift s = rint(M^-1 (c - p)) is chosen in fractional
+   coordinates and l = M s is taken off c when positive, added to p otherwise, per axis.
+   Every operation is written out (fma where the product is fused) so that the library's
+   kernels, which perform the same steps, produce the same doubles. */
+typedef struct {
+    double m11, m12, m21, m22;
+    double i11, i12, i21, i22;
+} gbox;
+
+static void gbox_init(gbox *g, const double *box)
+{
+    const double det = box[0] * box[3] - box[1] * box[2];
+    g->m11 = box[0];
+    g->m12 = box[1];
+    g->m21 = box[2];
+    g->m22 = box[3];
+    g->i11 = box[3] / det;
+    g->i12 = -box[1] / det;
+    g->i21 = -box[2] / det;
+    g->i22 = box[0] / det;
+}
+
+static inline double gen_off1(double c, double p, double l)
+{
+    return l >= 0.0 ? (c - l) - p : c - (p + l);
+}
+
+static inline d2 gen_offset(const gbox *g, d2 c, d2 p)
+{
+    const double dx = c.x - p.x, dy = c.y - p.y;
+    const double su = rint(fma(g->i11, dx, g->i12 * dy));
+    const double sv = rint(fma(g->i21, dx, g->i22 * dy));
+    const double lx = fma(g->m11, su, g->m12 * sv);
+    const double ly = fma(g->m21, su, g->m22 * sv);
+    d2 r;
+    r.x = gen_off1(c.x, p.x, lx);
+    r.y = gen_off1(c.y, p.y, ly);
+    return r;
+}
+
+void orc_offset_general(const double *c, const double *p, const double *box, double *out)
+{
+    gbox g;
+    gbox_init(&g, box);
+    d2 cc = { c[0], c[1] }, pp = { p[0], p[1] };
+    d2 r = gen_offset(&g, cc, pp);
+    out[0] = r.x;
+    out[1] = r.y;
+}
+
+/* Lagrange-Gauss reduction of the basis (columns (box[0], box[2]) and (box[1], box[3])), the
+   steps the library applies before using a general box */
+void orc_reduce_basis(double *box)
+{
+    double ax = box[0], ay = box[2], bx = box[1], by = box[3];
+    for (int it = 0; it < 64; ++it) {
+        if (ax * ax + ay * ay > bx * bx + by * by) {
+            double t = ax; ax = bx; bx = t;
+            t = ay; ay = by; by = t;
+        }
+        const double mu = nearbyint((ax * bx + ay * by) / (ax * ax + ay * ay));
+        if (mu == 0.0) break;
+        bx -= mu * ax;
+        by -= mu * ay;
+    }
+    box[0] = ax;
+    box[2] = ay;
+    box[1] = bx;
+    box[3] = by;
+}
+
 #define SPLITTER 134217729.0 /* 2^27 + 1 */
 
 static inline void two_sum(double a, double b, double *x, double *y)
@@ -638,13 +713,40 @@ typedef struct {
     int min_deg, max_deg;
 } orc_report;
 
-static inline d2 off_of(const d2 *pts, int c, int p, double Lx, double Ly)
+/* the box a verification runs in: rectangular (general == 0, Lx x Ly) or general (g) */
+typedef struct {
+    int general;
+    double Lx, Ly;
+    gbox g;
+} vbox;
+
+static inline d2 off_of(const d2 *pts, int c, int p, const vbox *B)
 {
+    if (B->general) return gen_offset(&B->g, pts[c], pts[p]);
     d2 r;
-    r.x = dgt_offset1(pts[c].x, pts[p].x, Lx);
-    r.y = dgt_offset1(pts[c].y, pts[p].y, Ly);
+    r.x = dgt_offset1(pts[c].x, pts[p].x, B->Lx);
+    r.y = dgt_offset1(pts[c].y, pts[p].y, B->Ly);
     return r;
 }
+
+/* bucket coordinates (cell units of a gx x gy grid) of a point: rectangular pts / L * g; a
+   general box's fractional coordinates wrapped into [0, 1) times g */
+static inline void bucket_pos(const vbox *B, d2 p, int gx, int gy, double *fx, double *fy)
+{
+    if (!B->general) {
+        *fx = p.x / B->Lx * gx;
+        *fy = p.y / B->Ly * gy;
+        return;
+    }
+    double u = fma(B->g.i11, p.x, B->g.i12 * p.y), v = fma(B->g.i21, p.x, B->g.i22 * p.y);
+    u -= floor(u);
+    v -= floor(v);
+    *fx = u * gx;
+    *fy = v * gy;
+}
+
+static int verify_impl(const d2 *pts, int n, const vbox *B, const int *tri, const int *nn, int stride,
+                       int global_scan, int threads, orc_report *rep);
 
 /* Exact check that (tri, nn) is the periodic Delaunay triangulation of pts.  A triangulation
    whose rings are mutually consistent, whose fan triangles are all positively oriented and
@@ -654,7 +756,35 @@ static inline d2 off_of(const d2 *pts, int c, int p, double Lx, double Ly)
 int orc_verify(const double *pts_, int n, double Lx, double Ly, const int *tri, const int *nn, int stride,
                int global_scan, int threads, orc_report *rep)
 {
-    const d2 *pts = (const d2 *)pts_;
+    vbox B;
+    memset(&B, 0, sizeof(B));
+    B.Lx = Lx;
+    B.Ly = Ly;
+    return verify_impl((const d2 *)pts_, n, &B, tri, nn, stride, global_scan, threads, rep);
+}
+
+/* the same for a general periodic box (box_in[0..3] = x11, x12, x21, x22; see gen_offset),
+   in its reduced basis (the same lattice; a reduced basis is left as it is) */
+int orc_verify_general(const double *pts_, int n, const double *box_in, const int *tri, const int *nn,
+                       int stride, int global_scan, int threads, orc_report *rep)
+{
+    double box[4] = { box_in[0], box_in[1], box_in[2], box_in[3] };
+    orc_reduce_basis(box);
+    vbox B;
+    memset(&B, 0, sizeof(B));
+    B.general = 1;
+    gbox_init(&B.g, box);
+    /* strip widths between opposite box edges, in place of Lx and Ly */
+    const double area = fabs(box[0] * box[3] - box[1] * box[2]);
+    B.Lx = area / hypot(box[1], box[3]);
+    B.Ly = area / hypot(box[0], box[2]);
+    return verify_impl((const d2 *)pts_, n, &B, tri, nn, stride, global_scan, threads, rep);
+}
+
+static int verify_impl(const d2 *pts, int n, const vbox *B, const int *tri, const int *nn, int stride,
+                       int global_scan, int threads, orc_report *rep)
+{
+    const double Lx = B->Lx, Ly = B->Ly;
     memset(rep, 0, sizeof(*rep));
     rep->min_deg = 1 << 30;
     long long sdeg = 0, bidx = 0, asym = 0, npos = 0, wind = 0, nld = 0, ntri = 0, intr = 0;
@@ -676,14 +806,18 @@ int orc_verify(const double *pts_, int n, double Lx, double Ly, const int *tri, 
         cpts = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
         int *fill = (int *)calloc((size_t)gx * gy, sizeof(int));
         for (int i = 0; i < n; ++i) {
-            int cx = (int)floor(pts[i].x / Lx * gx), cy = (int)floor(pts[i].y / Ly * gy);
+            double fx, fy;
+            bucket_pos(B, pts[i], gx, gy, &fx, &fy);
+            int cx = (int)floor(fx), cy = (int)floor(fy);
             cx = cx < 0 ? 0 : (cx >= gx ? gx - 1 : cx);
             cy = cy < 0 ? 0 : (cy >= gy ? gy - 1 : cy);
             cstart[cy * gx + cx + 1]++;
         }
         for (int c = 0; c < gx * gy; ++c) cstart[c + 1] += cstart[c];
         for (int i = 0; i < n; ++i) {
-            int cx = (int)floor(pts[i].x / Lx * gx), cy = (int)floor(pts[i].y / Ly * gy);
+            double fx, fy;
+            bucket_pos(B, pts[i], gx, gy, &fx, &fy);
+            int cx = (int)floor(fx), cy = (int)floor(fy);
             cx = cx < 0 ? 0 : (cx >= gx ? gx - 1 : cx);
             cy = cy < 0 ? 0 : (cy >= gy ? gy - 1 : cy);
             int c = cy * gx + cx;
@@ -719,7 +853,7 @@ int orc_verify(const double *pts_, int n, double Lx, double Ly, const int *tri, 
         /* orientation, winding, local Delaunay */
         d2 off[512];
         int mm = m < 512 ? m : 512;
-        for (int k = 0; k < mm; ++k) off[k] = off_of(pts, r[k], i, Lx, Ly);
+        for (int k = 0; k < mm; ++k) off[k] = off_of(pts, r[k], i, B);
         int cross = 0, allpos = 1;
         for (int k = 0; k < mm; ++k) {
             d2 a = off[k], b = off[(k + 1) % mm];
@@ -744,10 +878,27 @@ int orc_verify(const double *pts_, int n, double Lx, double Ly, const int *tri, 
             double rad = sqrt(qx * qx + qy * qy);
             if (!(rad == rad) || rad > 0.25 * (Lx < Ly ? Lx : Ly)) rad = 0.25 * (Lx < Ly ? Lx : Ly);
             double marg = rad * 1e-6 + 1e-9;
-            double ax = pts[i].x + qx - rad - marg, bx = pts[i].x + qx + rad + marg;
-            double ay = pts[i].y + qy - rad - marg, by = pts[i].y + qy + rad + marg;
-            int x0 = (int)floor(ax / Lx * gx), x1 = (int)floor(bx / Lx * gx);
-            int y0 = (int)floor(ay / Ly * gy), y1 = (int)floor(by / Ly * gy);
+            int x0, x1, y0, y1;
+            if (!B->general) {
+                double ax = pts[i].x + qx - rad - marg, bx = pts[i].x + qx + rad + marg;
+                double ay = pts[i].y + qy - rad - marg, by = pts[i].y + qy + rad + marg;
+                x0 = (int)floor(ax / Lx * gx);
+                x1 = (int)floor(bx / Lx * gx);
+                y0 = (int)floor(ay / Ly * gy);
+                y1 = (int)floor(by / Ly * gy);
+            } else {
+                /* the circle's bounding box in bucket units: its centre's wrapped position,
+                   half extents (rad + marg) times the rows of diag(gx, gy) M^-1 */
+                d2 cen = { pts[i].x + qx, pts[i].y + qy };
+                double fx, fy;
+                bucket_pos(B, cen, gx, gy, &fx, &fy);
+                const double hu = (rad + marg) * gx * hypot(B->g.i11, B->g.i12) * (1 + 1e-9) + 1e-9;
+                const double hv = (rad + marg) * gy * hypot(B->g.i21, B->g.i22) * (1 + 1e-9) + 1e-9;
+                x0 = (int)floor(fx - hu);
+                x1 = (int)floor(fx + hu);
+                y0 = (int)floor(fy - hv);
+                y1 = (int)floor(fy + hv);
+            }
             if (x1 - x0 + 1 > gx) { x0 = 0; x1 = gx - 1; }
             if (y1 - y0 + 1 > gy) { y0 = 0; y1 = gy - 1; }
             int found = 0;
@@ -758,7 +909,7 @@ int orc_verify(const double *pts_, int n, double Lx, double Ly, const int *tri, 
                     for (int t = cstart[c]; t < cstart[c + 1]; ++t) {
                         int e = cpts[t];
                         if (e == i || e == y || e == z) continue;
-                        d2 de = off_of(pts, e, i, Lx, Ly);
+                        d2 de = off_of(pts, e, i, B);
                         if (orc_incircle0(&a.x, &b.x, &de.x) > 0) { found = 1; break; }
                     }
                 }

@@ -89,6 +89,13 @@ def lib():
         L.orc_orient0.argtypes = [_P_D, _P_D]
         L.orc_offset.restype = None
         L.orc_offset.argtypes = [_P_D, _P_D, ctypes.c_double, ctypes.c_double, _P_D]
+        L.orc_offset_general.restype = None
+        L.orc_offset_general.argtypes = [_P_D, _P_D, _P_D, _P_D]
+        L.orc_reduce_basis.restype = None
+        L.orc_reduce_basis.argtypes = [_P_D]
+        L.orc_verify_general.restype = ctypes.c_int
+        L.orc_verify_general.argtypes = [_P_D, ctypes.c_int, _P_D, _P_I, _P_I, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_int, ctypes.POINTER(OrcReport)]
         L.orc_canonical_rotate.restype = None
         L.orc_canonical_rotate.argtypes = [_P_I, _P_I, ctypes.c_int, ctypes.c_int]
         _lib = L
@@ -261,6 +268,36 @@ def verify(points, Lx, Ly, tri, nn, global_scan=True, threads=None):
     r = lib().orc_verify(_pd(pts), len(pts), Lx, Ly, _pi(t), _pi(nnv), t.shape[1], 1 if global_scan else 0,
                          threads or default_threads(), ctypes.byref(rep))
     return r == 0, rep.as_dict()
+
+
+def verify_general(points, box, tri, nn, global_scan=True, threads=None):
+    """verify() in a general periodic box, box = (xx, xy, yx, yy) (periodicBoundaries(a, b, c, d);
+    lattice vectors (xx, yx) and (xy, yy)).  Returns (ok, report dict)."""
+    pts = _prep(points)
+    bx = np.ascontiguousarray(box, dtype=np.float64)
+    t = np.ascontiguousarray(tri, dtype=np.int32)
+    nnv = np.ascontiguousarray(nn, dtype=np.int32)
+    rep = OrcReport()
+    r = lib().orc_verify_general(_pd(pts), len(pts), _pd(bx), _pi(t), _pi(nnv), t.shape[1],
+                                 1 if global_scan else 0, threads or default_threads(), ctypes.byref(rep))
+    return r == 0, rep.as_dict()
+
+
+def offset_general(c, p, box):
+    """Offset c - p to the image whose fractional offset lies in [-1/2, 1/2] (general box)."""
+    c = np.ascontiguousarray(c, np.float64)
+    p = np.ascontiguousarray(p, np.float64)
+    bx = np.ascontiguousarray(box, np.float64)
+    out = np.zeros(2, np.float64)
+    lib().orc_offset_general(_pd(c), _pd(p), _pd(bx), _pd(out))
+    return out
+
+
+def reduce_basis(box):
+    """Lagrange-Gauss reduced basis of the lattice of box = (xx, xy, yx, yy)."""
+    bx = np.array(box, dtype=np.float64)
+    lib().orc_reduce_basis(_pd(bx))
+    return tuple(float(v) for v in bx)
 
 
 def canonical(tri, nn):

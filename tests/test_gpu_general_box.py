@@ -1,0 +1,153 @@
+"""General (non-rectangular) periodic boxes on the GPU (dgt_set_box_general).
+
+The reference's box class supports general boxes (periodicBoundaries.h:86-101, 165-178) but
+its cell list and Delaunay kernels do not (cellListGPU.h:14-16), so there is no reference
+output to compare with.  Parity is anchored instead on the rectangular path, which matches the
+reference bit for bit: a rotated rectangle and a sheared basis of a rectangular lattice must
+give the same rings, and in genuinely oblique boxes every result must pass the oracle's exact
+verifier (rings mutually consistent, CCW, winding once, every edge locally Delaunay, every
+circumcircle empty under a global scan), which for points in general position pins the unique
+Delaunay triangulation."""
+import math
+
+import numpy as np
+import pytest
+
+from gpudelaunaytriangulation_b200 import workloads as W
+from oracle import oracle as O
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+def _dgpu():
+    from gpudelaunaytriangulation_b200.delaunay import DelaunayGPU, PeriodicBox
+
+    return DelaunayGPU, PeriodicBox
+
+
+def _build(pts, box, cell=1.0, fp32=True):
+    DelaunayGPU, _ = _dgpu()
+    n = len(pts)
+    d = DelaunayGPU(n, 16, cell, box)
+    d.setPrecision(fp32)
+    P = torch.from_numpy(np.ascontiguousarray(pts)).cuda()
+    tri, nn = d.globalDelaunayTriangulation(P)
+    torch.cuda.synchronize()
+    t = tri.view(n, -1).cpu().numpy()
+    k = nn.cpu().numpy()
+    return d, P, tri, nn, t, k
+
+
+def _same_rings(t0, k0, t1, k1):
+    w = min(t0.shape[1], t1.shape[1])
+    return np.array_equal(k0, k1) and np.array_equal(O.canonical(t0, k0)[:, :w], O.canonical(t1, k1)[:, :w])
+
+
+def _oblique_points(n, box, seed):
+    M = np.array([[box[0], box[1]], [box[2], box[3]]])
+    u = np.random.default_rng(seed).uniform(0.0, 1.0, (n, 2))
+    return np.ascontiguousarray(u @ M.T)
+
+
+def _box_of_area(n, shape):
+    # scale a box shape (xx, xy, yx, yy) to unit density for n points
+    det = abs(shape[0] * shape[3] - shape[1] * shape[2])
+    s = math.sqrt(n / det)
+    return tuple(s * v for v in shape)
+
+
+HEX = (1.0, 0.5, 0.0, math.sqrt(3.0) / 2.0)   # 60-degree lattice
+OBLIQUE = (40.0, 13.0, 3.0, 35.0)              # an arbitrary oblique lattice
+
+
+@pytest.mark.parametrize("theta", [0.37, 1.1])
+def test_rotated_rectangle_matches_the_rectangular_path(theta):
+    n = 20000
+    L = math.sqrt(n)
+    pts = W.uniform_points(n, L, 41)
+    _, _, _, _, t0, k0 = _build(pts, (L, L))
+    R = np.array([[math.cos(theta), -math.sin(theta)], [math.sin(theta), math.cos(theta)]])
+    box = R @ np.diag([L, L])
+    rbox = (box[0, 0], box[0, 1], box[1, 0], box[1, 1])
+    d, P, tri, nn, t1, k1 = _build(pts @ R.T, rbox)
+    st = d.stats()
+    assert st["error_flags"] == 0 and st["mismatches"] == 0, st
+    assert _same_rings(t0, k0, t1, k1)
+    assert d.validate(P, tri, nn)["valid"] == 1
+    ok, rep = O.verify_general(pts @ R.T, d.kernelBox(), t1, k1)
+    assert ok, rep
+
+
+def test_sheared_basis_of_a_rectangular_lattice_and_shifted_images():
+    n = 20000
+    L = math.sqrt(n)
+    pts = W.uniform_points(n, L, 42)
+    _, _, _, _, t0, k0 = _build(pts, (L, L))
+    # lattice vectors (L, 0) and (2L, L): the square lattice through a sheared basis
+    DelaunayGPU, PeriodicBox = _dgpu()
+    d, P, tri, nn, t1, k1 = _build(pts, PeriodicBox.general(L, 2 * L, 0.0, L))
+    kb = d.kernelBox()
+    assert abs(abs(kb[0] * kb[3] - kb[1] * kb[2]) - L * L) < 1e-9 * L * L
+    assert _same_rings(t0, k0, t1, k1)
+    # every point moved by a lattice vector: the same periodic point set
+    shifted = pts + np.outer(np.arange(n) % 5 - 2, [L, 0.0]) + np.outer(np.arange(n) % 3 - 1, [2 * L, L])
+    _, _, _, _, t2, k2 = _build(shifted, (L, 2 * L, 0.0, L))
+    assert _same_rings(t0, k0, t2, k2)
+
+
+@pytest.mark.parametrize("shape", [HEX, OBLIQUE], ids=["hex", "oblique"])
+def test_oblique_box_is_delaunay_in_both_precisions(shape):
+    n = 30000
+    box = _box_of_area(n, shape)
+    pts = _oblique_points(n, box, 43)
+    d, P, tri, nn, t, k = _build(pts, box)
+    st = d.stats()
+    assert st["error_flags"] == 0 and st["mismatches"] == 0, st
+    assert int(k.sum()) == 6 * n
+    assert d.validate(P, tri, nn)["valid"] == 1
+    ok, rep = O.verify_general(pts, d.kernelBox(), t, k)
+    assert ok, rep
+    _, _, _, _, t64, k64 = _build(pts, box, fp32=False)
+    assert _same_rings(t, k, t64, k64)
+
+
+@pytest.mark.parametrize("flip", [True, False], ids=["flips", "rebuild"])
+def test_oblique_box_repair_matches_a_fresh_build(flip):
+    n = 30000
+    box = _box_of_area(n, OBLIQUE)
+    pts = _oblique_points(n, box, 44)
+    d, P, tri, nn, _, _ = _build(pts, box)
+    d.setFlipRepair(flip)
+    rng = np.random.default_rng(45)
+    for step in range(3):
+        pts = pts + rng.normal(0.0, 0.05, pts.shape)   # left unwrapped: any position is valid
+        P.copy_(torch.from_numpy(pts))
+        d.testAndRepairDelaunayTriangulation(P, tri, nn)
+        torch.cuda.synchronize()
+        assert d.stats()["error_flags"] == 0
+    t = tri.view(n, -1).cpu().numpy()
+    k = nn.cpu().numpy()
+    _, _, _, _, tf, kf = _build(pts, box)
+    assert _same_rings(t, k, tf, kf)
+    ok, rep = O.verify_general(pts, d.kernelBox(), t, k)
+    assert ok, rep
+
+
+def test_oblique_box_md_steps_wrap_into_the_unit_cell():
+    n = 20000
+    box = _box_of_area(n, HEX)
+    pts = _oblique_points(n, box, 46)
+    d, P, tri, nn, _, _ = _build(pts, box)
+    for _ in range(5):
+        d.mdStep(P, tri, nn, 0.02, 47)
+    torch.cuda.synchronize()
+    assert d.stats()["error_flags"] == 0
+    q = P.cpu().numpy()
+    kb = d.kernelBox()
+    Mi = np.linalg.inv(np.array([[kb[0], kb[1]], [kb[2], kb[3]]]))
+    u = q @ Mi.T
+    assert np.all(u >= -1e-9) and np.all(u < 1.0 + 1e-9)
+    assert d.validate(P, tri, nn)["valid"] == 1
+    ok, rep = O.verify_general(q, kb, tri.view(n, -1).cpu().numpy(), nn.cpu().numpy())
+    assert ok, rep
