@@ -17,6 +17,7 @@
 
 #include <cuda_runtime_api.h>
 
+#include <cmath>
 #include <cstddef>
 #include <stdexcept>
 #include <string>
@@ -92,8 +93,20 @@ class DelaunayGPU {
     {
         double xx, xy, yx, yy;
         (*box).getBoxDims(xx, xy, yx, yy);
-        if (xy != 0.0 || yx != 0.0) throw std::invalid_argument("DelaunayGPU: only rectangular boxes");
-        check(dgt_create(N, maximumNeighborsGuess, cellSize, xx, yy, &ctx_), "dgt_create");
+        if (xy == 0.0 && yx == 0.0) {
+            check(dgt_create(N, maximumNeighborsGuess, cellSize, xx, yy, &ctx_), "dgt_create");
+            return;
+        }
+        // a general box (periodicBoundaries::setGeneral): created on the bounding rectangle,
+        // then given the box matrix
+        check(dgt_create(N, maximumNeighborsGuess, cellSize, std::fabs(xx) + std::fabs(xy),
+                         std::fabs(yx) + std::fabs(yy), &ctx_), "dgt_create");
+        const int rc = dgt_set_box_general(ctx_, xx, xy, yx, yy);
+        if (rc != DGT_OK) {
+            dgt_destroy(ctx_);
+            ctx_ = nullptr;
+            check(rc, "setBox");
+        }
     }
     DelaunayGPU(const DelaunayGPU &) = delete;
     DelaunayGPU &operator=(const DelaunayGPU &) = delete;
@@ -153,6 +166,15 @@ class DelaunayGPU {
     void resize(int nmax) { check(dgt_resize(ctx_, nmax), "resize"); }
     void setCellListSize(double csize) { check(dgt_set_cell_size(ctx_, csize), "setCellListSize"); }
     void setBox(double Lx, double Ly) { check(dgt_set_box(ctx_, Lx, Ly), "setBox"); }
+    // setBox(bx) (DelaunayGPU.h:44) with any box type with getBoxDims, rectangular or general
+    template <class BoxPtr>
+    void setBox(const BoxPtr &box)
+    {
+        double xx, xy, yx, yy;
+        (*box).getBoxDims(xx, xy, yx, yy);
+        if (xy == 0.0 && yx == 0.0) check(dgt_set_box(ctx_, xx, yy), "setBox");
+        else check(dgt_set_box_general(ctx_, xx, xy, yx, yy), "setBox");
+    }
     void setSafetyMode(bool on)
     {
         safety_ = on;

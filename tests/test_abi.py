@@ -55,13 +55,21 @@ def test_invalid_arguments_without_device():
     v = ctypes.c_int()
     assert L.dgt_get_max_size(None, ctypes.byref(v)) == N.DGT_ERR_INVALID_ARGUMENT
     assert L.dgt_restride(None, 4, None, 8, None, 5, None) == N.DGT_ERR_INVALID_ARGUMENT
+    assert L.dgt_set_box_general(None, 1.0, 0.5, 0.0, 1.0) == N.DGT_ERR_INVALID_ARGUMENT
+    box = (ctypes.c_double * 4)()
+    assert L.dgt_get_box(None, box) == N.DGT_ERR_INVALID_ARGUMENT
     L.dgt_destroy(None)
 
 
 @pytest.mark.skipif(shutil.which("g++") is None, reason="no host C++ compiler")
 def test_cpp_adapter_header_compiles(tmp_path):
     src = tmp_path / "use.cpp"
-    src.write_text('#include "dgt_delaunay.hpp"\nint main(){ return 0; }\n')
+    # the box-object constructor and setBox instantiated with a general box type
+    src.write_text('#include <memory>\n#include "dgt_delaunay.hpp"\n'
+                   'struct Box { void getBoxDims(double &a, double &b, double &c, double &d) const '
+                   '{ a = 10; b = 5; c = 0; d = 8; } };\n'
+                   'void use() { auto bx = std::make_shared<Box>(); dgt::DelaunayGPU g(100, 16, 1.0, bx); '
+                   'g.setBox(bx); }\nint main(){ return 0; }\n')
     cuda_inc = "/usr/local/cuda/include"
     r = subprocess.run(["g++", "-std=c++14", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), "-I", cuda_inc,
                         str(src)], capture_output=True, text=True)
