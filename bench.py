@@ -310,7 +310,8 @@ def _timed_call(fn, stream=None):
 def configs_measure(dev):
     """The other workload families, each measured once (not the headline): 1M points with 20
     float64 repair steps; 1M-site jittered triangular lattice and 1M-point 64-cluster Gaussian
-    mixture (float32 filter, autotuned settings, check mode for mismatches)."""
+    mixture (float32 filter, autotuned settings, check mode for mismatches); 1M points in a
+    general (60-degree) periodic box."""
     import torch
 
     from gpudelaunaytriangulation_b200.delaunay import DelaunayGPU
@@ -359,6 +360,37 @@ def configs_measure(dev):
                      "mismatches": st["mismatches"], "flags": st["error_flags"], "max_ring": st["max_ring"],
                      "sum_ring_sizes_is_6n": int(nn[: n].sum().item()) == 6 * n}
         d.close()
+    # general periodic box: 1,048,576 uniform points in a 60-degree box at unit density, float32
+    # filter; build, one repair after a sigma = 0.02 displacement, device validation
+    n = 1 << 20
+    s = float(np.sqrt(n / (np.sqrt(3.0) / 2.0)))
+    box = (s, 0.5 * s, 0.0, s * np.sqrt(3.0) / 2.0)
+    M = np.array([[box[0], box[1]], [box[2], box[3]]])
+    hp = np.ascontiguousarray(np.random.default_rng(61).uniform(0.0, 1.0, (n, 2)) @ M.T)
+    P = torch.from_numpy(hp).to(dev)
+    d = DelaunayGPU(n, 16, 1.0, box)
+    tri = torch.zeros(16 * n, dtype=torch.int32, device=dev)
+    nn = torch.zeros(n, dtype=torch.int32, device=dev)
+    d.globalDelaunayTriangulation(P, tri, nn)
+    b_ms = _timed_call(lambda: d.globalDelaunayTriangulation(P, tri, nn))
+    # repair steps: sigma = 0.02 per axis, left unwrapped (any position is valid in a general
+    # box); one warm-up step, then 5 timed ones (displacements drawn outside the timed calls)
+    gen = torch.Generator(device=dev).manual_seed(62)
+    r_ms, rep = [], []
+    for k in range(6):
+        P.add_(torch.randn(P.shape, generator=gen, device=dev, dtype=torch.float64), alpha=0.02)
+        ms = _timed_call(lambda: d.testAndRepairDelaunayTriangulation(P, tri, nn))
+        if k > 0:
+            r_ms.append(ms)
+            rep.append(d.stats()["repaired"])
+    st = d.stats()
+    v = d.validate(P, tri, nn)
+    rm = float(np.mean(r_ms))
+    out["hex_box_1m_fp32"] = {"points": n, "box": [float(x) for x in d.kernelBox()], "build_ms": b_ms,
+                              "build_mpts": n / b_ms / 1e3, "repair_step_ms": rm, "repair_step_mpts": n / rm / 1e3,
+                              "repaired_per_step": float(np.mean(rep)), "flags": st["error_flags"],
+                              "valid": v["valid"]}
+    d.close()
     return out
 
 
