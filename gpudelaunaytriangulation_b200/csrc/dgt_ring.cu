@@ -306,7 +306,9 @@ struct Builder {
         // than the positions (cell lists kept from the last binning)
         const bool by_index = CAND == 1 || (CAND == 2 && A.cand_by_index);
         double2 q = by_index ? __ldg(&A.pos[__ldg(&A.sidx[sl])]) : __ldg(&A.spos[sl]);
-        double2 d64 = GEN ? gen_off(q, p, S)
+        // general box: the matrices are read through the descriptor in global memory (L1
+        // hits) rather than held in registers across the scan
+        double2 d64 = GEN ? gen_off(q, p, *Sg)
                           : make_double2(wrap_off(q.x, p.x, S.Lx, S.hLx), wrap_off(q.y, p.y, S.Ly, S.hLy));
         if (d64.x == 0.0 && d64.y == 0.0) return R_OK;   // coincident point
         ctr.cand++;
