@@ -33,7 +33,7 @@ EXPORTED = [
     "dgt_get_phase_times", "dgt_global_triangulation_noalloc", "dgt_md_step", "dgt_md_graph_create",
     "dgt_md_graph_launch", "dgt_md_graph_destroy", "dgt_clear_flags", "dgt_set_kernel_shape",
     "dgt_get_tuning", "dgt_autotune", "dgt_set_work_budget", "dgt_set_flip_repair",
-    "dgt_validate", "dgt_get_cell_order", "dgt_set_box_general", "dgt_get_box",
+    "dgt_validate", "dgt_get_cell_order", "dgt_set_box_general", "dgt_get_box", "dgt_create_batch_general",
 ]
 STEP_AUTO = 0xFFFFFFFFFFFFFFFF
 NOALLOC_MAX_POINTS = 65536
@@ -136,6 +136,8 @@ def lib() -> ctypes.CDLL:
     L.dgt_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                              ctypes.POINTER(vp)]
     L.dgt_create_batch.argtypes = [ctypes.c_int, P_I, P_D, ctypes.c_double, ctypes.c_int, ctypes.POINTER(vp)]
+    L.dgt_create_batch_general.argtypes = [ctypes.c_int, P_I, P_D, ctypes.c_double, ctypes.c_int,
+                                           ctypes.POINTER(vp)]
     L.dgt_destroy.argtypes = [vp]
     L.dgt_destroy.restype = None
     L.dgt_global_triangulation.argtypes = [vp, vp, vp, vp, ctypes.c_int, vp]

@@ -67,10 +67,11 @@ struct dgt_context {
     bool batch = false;
     std::vector<int> sizes;
     std::vector<double> boxes;
-    // general periodic box (single-set contexts): the reduced basis the kernels use, columns
-    // (gbox[0], gbox[2]) and (gbox[1], gbox[3]); boxes then holds its bounding rectangle
+    // general periodic boxes: per set the reduced basis the kernels use (4 values, columns
+    // (g[0], g[2]) and (g[1], g[3])); boxes then holds each set's bounding rectangle.  A
+    // rectangular set of a general batch is the diagonal matrix.
     int general = 0;
-    double gbox[4] = { 0, 0, 0, 0 };
+    std::vector<double> gboxes;
     double cell_size = 1.0;
     int max_size = 16;
     int safety = 1;
@@ -232,9 +233,13 @@ int plan_grid(dgt_context *c)
         double Lx = c->boxes[2 * s], Ly = c->boxes[2 * s + 1];
         int ns = c->sizes[s];
         if (c->general) {
-            const double area = std::fabs(c->gbox[0] * c->gbox[3] - c->gbox[1] * c->gbox[2]);
+            const double *g = &c->gboxes[4 * s];
+            const double spacing = std::sqrt(std::fabs(g[0] * g[3] - g[1] * g[2]) / std::max(ns, 1));
+            double a;
+            if (c->batch) a = (c->cell_size > 0 ? c->cell_size : 1.0) * spacing;
+            else a = c->cell_size > 0 ? c->cell_size : spacing;
             SetDesc &S = c->sets[s];
-            plan_general_set(S, c->gbox, c->cell_size > 0 ? c->cell_size : std::sqrt(area / std::max(ns, 1)), ns);
+            plan_general_set(S, g, a, ns);
             S.cell_base = (int)cells;
             S.point_base = pbase;
             S.n = ns;
@@ -518,6 +523,48 @@ int dgt_create(int n, int max_neighs, double cell_size, double Lx, double Ly, dg
     return DGT_OK;
 }
 
+int dgt_create_batch_general(int num_sets, const int *sizes, const double *boxes4, double cell_size, int max_neighs,
+                             dgt_context **out)
+{
+    if (!out) return DGT_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (num_sets <= 0 || !sizes || !boxes4 || !std::isfinite(cell_size)) return DGT_ERR_INVALID_ARGUMENT;
+    long long total = 0;
+    std::vector<double> g(boxes4, boxes4 + 4 * (size_t)num_sets), rect(2 * (size_t)num_sets);
+    for (int s = 0; s < num_sets; ++s) {
+        double *b = &g[4 * (size_t)s];
+        bool finite = true;
+        for (int k = 0; k < 4; ++k) finite &= std::isfinite(b[k]);
+        const double det = b[0] * b[3] - b[1] * b[2];
+        const double scale = (std::fabs(b[0]) + std::fabs(b[2])) * (std::fabs(b[1]) + std::fabs(b[3]));
+        if (sizes[s] < 0 || !finite || !(std::fabs(det) > 1e-12 * scale)) return DGT_ERR_INVALID_ARGUMENT;
+        reduce_basis(b);
+        rect[2 * s] = std::fabs(b[0]) + std::fabs(b[1]);
+        rect[2 * s + 1] = std::fabs(b[2]) + std::fabs(b[3]);
+        total += sizes[s];
+    }
+    if (total > (1LL << 30)) return DGT_ERR_INVALID_ARGUMENT;
+    dgt_context *c = new (std::nothrow) dgt_context();
+    if (!c) return DGT_ERR_OUT_OF_MEMORY;
+    cudaGetDevice(&c->device);
+    c->batch = true;
+    c->num_sets = num_sets;
+    c->n = (int)total;
+    c->sizes.assign(sizes, sizes + num_sets);
+    c->boxes = rect;
+    c->general = 1;
+    c->gboxes = g;
+    c->cell_size = cell_size;
+    c->max_size = std::max(4, max_neighs);
+    int r = init_context(c);
+    if (r != DGT_OK) {
+        dgt_destroy(c);
+        return r;
+    }
+    *out = c;
+    return DGT_OK;
+}
+
 int dgt_create_batch(int num_sets, const int *sizes, const double *boxes, double cell_size, int max_neighs,
                      dgt_context **out)
 {
@@ -788,7 +835,7 @@ int dgt_set_box_general(dgt_context *c, double x11, double x12, double x21, doub
     if (x12 == 0.0 && x21 == 0.0 && x11 > 0.0 && x22 > 0.0) return dgt_set_box(c, x11, x22);
     double g[4] = { x11, x12, x21, x22 };
     reduce_basis(g);
-    std::memcpy(c->gbox, g, sizeof(g));
+    c->gboxes.assign(g, g + 4);
     c->general = 1;
     c->boxes = { std::fabs(g[0]) + std::fabs(g[1]), std::fabs(g[2]) + std::fabs(g[3]) };
     return init_context(c);
@@ -798,7 +845,7 @@ int dgt_get_box(const dgt_context *c, double *out4)
 {
     if (!c || !out4 || c->batch) return DGT_ERR_INVALID_ARGUMENT;
     if (c->general) {
-        std::memcpy(out4, c->gbox, sizeof(c->gbox));
+        std::memcpy(out4, c->gboxes.data(), sizeof(double) * 4);
     } else {
         out4[0] = c->boxes[0];
         out4[1] = 0.0;
@@ -1088,7 +1135,7 @@ int ilog2(long long v)
 // mean spacing of a single-set context (cell sizes are absolute there)
 double spacing_of(const dgt_context *c)
 {
-    const double area = c->general ? std::fabs(c->gbox[0] * c->gbox[3] - c->gbox[1] * c->gbox[2])
+    const double area = c->general ? std::fabs(c->gboxes[0] * c->gboxes[3] - c->gboxes[1] * c->gboxes[2])
                                    : c->boxes[0] * c->boxes[1];
     return std::sqrt(area / std::max(c->n, 1));
 }

@@ -115,9 +115,16 @@ class DelaunayGPU:
         if _batch is not None:
             sizes, boxes, rel_cell = _batch
             sz = (ctypes.c_int * len(sizes))(*[int(s) for s in sizes])
-            bx = (ctypes.c_double * (2 * len(sizes)))(*[float(v) for b in boxes for v in b])
-            _nat.check(lib.dgt_create_batch(len(sizes), sz, bx, float(rel_cell), int(maximumNeighborsGuess),
-                                           ctypes.byref(self._h)), "dgt_create_batch")
+            pb = [PeriodicBox.of(b) for b in boxes]
+            if all(b.isBoxSquare() for b in pb):
+                bx = (ctypes.c_double * (2 * len(sizes)))(*[v for b in pb for v in (b.Lx, b.Ly)])
+                _nat.check(lib.dgt_create_batch(len(sizes), sz, bx, float(rel_cell), int(maximumNeighborsGuess),
+                                               ctypes.byref(self._h)), "dgt_create_batch")
+            else:
+                bx = (ctypes.c_double * (4 * len(sizes)))(*[v for b in pb for v in b.getBoxDims()])
+                _nat.check(lib.dgt_create_batch_general(len(sizes), sz, bx, float(rel_cell),
+                                                       int(maximumNeighborsGuess), ctypes.byref(self._h)),
+                           "dgt_create_batch_general")
             self.Ncells = int(sum(int(s) for s in sizes))
             self.Box = None
         else:
@@ -408,4 +415,4 @@ class DelaunayBatch(DelaunayGPU):
     def __init__(self, sizes, boxes, maximumNeighborsGuess: int = 16, cellSizeRelative: float = 1.0):
         super().__init__(0, maximumNeighborsGuess, 0.0, None, _batch=(list(sizes), list(boxes), cellSizeRelative))
         self.sizes = [int(s) for s in sizes]
-        self.boxes = [(float(b[0]), float(b[1])) for b in boxes]
+        self.boxes = [PeriodicBox.of(b) for b in boxes]

@@ -9,7 +9,8 @@
  * Output layout (same as the reference, DelaunayGPU.cpp:47 Index2D(MaxSize, N)):
  *   tri[i*stride + k], k < neighnum[i]: indices of the Delaunay neighbours of point i in
  *   counter-clockwise order; rows start at the smallest neighbour index.
- * Points: double2[n] as 2n doubles (x0,y0,x1,y1,...), every coordinate in [0, L) of its box.
+ * Points: double2[n] as 2n doubles (x0,y0,x1,y1,...), every coordinate in [0, L) of its box
+ * (any finite coordinates in a general box, dgt_set_box_general).
  * All pointers named d_* are device pointers on the context's device; `stream` is a
  * cudaStream_t (NULL = legacy default stream).
  * Contexts are not thread-safe (like the reference class); use one per host thread.
@@ -96,6 +97,11 @@ int dgt_create(int n, int max_neighs, double cell_size, double Lx, double Ly, dg
  * counterpart: the reference triangulates one set per DelaunayGPU object. */
 int dgt_create_batch(int num_sets, const int *sizes, const double *boxes, double cell_size, int max_neighs,
                      dgt_context **out);
+/* dgt_create_batch with general periodic boxes: boxes4 holds (xx, xy, yx, yy) per set, as
+ * dgt_set_box_general (a rectangle is (Lx, 0, 0, Ly)); each basis is reduced.  No reference
+ * counterpart (see dgt_create_batch and dgt_set_box_general). */
+int dgt_create_batch_general(int num_sets, const int *sizes, const double *boxes4, double cell_size, int max_neighs,
+                             dgt_context **out);
 
 void dgt_destroy(dgt_context *ctx);
 

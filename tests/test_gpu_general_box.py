@@ -151,3 +151,49 @@ def test_oblique_box_md_steps_wrap_into_the_unit_cell():
     assert d.validate(P, tri, nn)["valid"] == 1
     ok, rep = O.verify_general(q, kb, tri.view(n, -1).cpu().numpy(), nn.cpu().numpy())
     assert ok, rep
+
+
+def test_batch_of_general_and_rectangular_boxes_matches_single_sets():
+    from gpudelaunaytriangulation_b200.delaunay import DelaunayBatch
+
+    rng = np.random.default_rng(48)
+    hexb = _box_of_area(5000, HEX)
+    obl = _box_of_area(3000, OBLIQUE)
+    Lr = math.sqrt(4000)
+    th = 0.6
+    R = np.array([[math.cos(th), -math.sin(th)], [math.sin(th), math.cos(th)]]) @ np.diag([math.sqrt(2000)] * 2)
+    rot = (R[0, 0], R[0, 1], R[1, 0], R[1, 1])
+    sizes = [5000, 3000, 4000, 0, 2000]
+    boxes = [hexb, obl, (Lr, Lr), (10.0, 10.0), rot]
+    sets = [_oblique_points(5000, hexb, 49), _oblique_points(3000, obl, 50), W.uniform_points(4000, Lr, 51),
+            np.zeros((0, 2)), _oblique_points(2000, rot, 52)]
+    pts = np.ascontiguousarray(np.concatenate(sets))
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    b = DelaunayBatch(sizes, boxes, 16, 1.0)
+    P = torch.from_numpy(pts).cuda()
+    for step in range(2):
+        if step == 1:
+            # drift every set, then repair the batch in place
+            pts = pts + rng.normal(0.0, 0.03, pts.shape)
+            sets = [pts[off[s]:off[s + 1]] for s in range(len(sizes))]
+            P.copy_(torch.from_numpy(pts))
+            b.testAndRepairDelaunayTriangulation(P, tri, nn)
+        else:
+            tri, nn = b.globalDelaunayTriangulation(P)
+        torch.cuda.synchronize()
+        assert b.stats()["error_flags"] == 0
+        t = tri.view(len(pts), -1).cpu().numpy()
+        k = nn.cpu().numpy()
+        for s in range(len(sizes)):
+            lo, hi = off[s], off[s + 1]
+            if hi == lo:
+                continue
+            ts = t[lo:hi].copy()
+            ts[np.arange(ts.shape[1])[None, :] < k[lo:hi, None]] -= lo
+            box = boxes[s] if len(boxes[s]) == 4 else (boxes[s][0], 0.0, 0.0, boxes[s][1])
+            if len(boxes[s]) == 2:
+                sets[s] = np.mod(sets[s], Lr)   # the single-set rectangular path wants [0, L)
+            _, _, _, _, t1, k1 = _build(sets[s], boxes[s])
+            assert _same_rings(ts, k[lo:hi], t1, k1), (step, s)
+            ok, rep = O.verify_general(sets[s], box, ts, k[lo:hi])
+            assert ok, (step, s, rep)
