@@ -54,7 +54,7 @@ struct DevBuf {
 constexpr int FIRST_ROUNDS = 3;     // repair rounds launched before the first host check
 constexpr int NEXT_ROUNDS = 2;      // rounds per later batch (each kernel exits at once on an empty list)
 constexpr int ASYNC_ROUNDS = 6;     // rounds of an unsynchronised call (convergence flagged on the device)
-constexpr int FLIP_BATCH = 4;       // flip rounds launched before each host check
+constexpr int FLIP_BATCH = 12;      // flip rounds launched before each host check (empty rounds exit at once)
 constexpr int MAX_FLIP_ROUNDS = 24; // flip rounds of a checked call before the rest is rebuilt
 constexpr int ASYNC_FLIP_ROUNDS = 6; // flip rounds of an unsynchronised call
 
@@ -725,7 +725,6 @@ int repair_impl(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, i
                 f.cur_count = &dst->flip_count[fr & 1];
                 f.next = flips[(fr + 1) & 1];
                 f.next_count = &dst->flip_count[(fr + 1) & 1];
-                DGT_TRY(cudaMemsetAsync(f.next_count, 0, sizeof(int), s));
                 c->launches += 2;
                 DGT_TRY(launch_flip_round(f, fr, c->sms, s));
             }

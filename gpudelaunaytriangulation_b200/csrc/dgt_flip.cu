@@ -136,6 +136,9 @@ __global__ void __launch_bounds__(256, 2) k_flip_claim(FlipArgs A, int round)
     const int ebase = *A.epoch_ptr + 1;
     const unsigned stamp = *A.stamp_ptr + 1 + round;
     const int n = min(*A.cur_count, A.cap);
+    // the next round's list is appended by this round's apply kernel: cleared here (the last
+    // reader of that buffer, the previous round's apply, has finished) instead of by a memset
+    if (blockIdx.x == 0 && threadIdx.x == 0) *A.next_count = 0;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
         const int2 ed = A.cur[e];
         const int i = ed.x, j = ed.y;
