@@ -166,11 +166,14 @@ __global__ void __launch_bounds__(256) k_scatter(BinArgs a)
     if (i >= a.n) return;
     int slot = a.cstart[a.cell_of[i]] + a.rank[i];
     a.sidx[slot] = i;
-    a.spos[slot] = a.pos[i];
-    if (!a.deterministic) a.slot_of[i] = slot;
+    if (!a.deterministic) {
+        a.spos[slot] = a.pos[i];
+        a.slot_of[i] = slot;
+    }
 }
 
-// per cell: order its points by index (insertion sort; cells hold a handful of points)
+// per cell: order its points by index (insertion sort of the indices; cells hold a handful
+// of points), then the cell-order positions, written once and contiguously per cell
 __global__ void __launch_bounds__(256) k_cell_order(BinArgs a)
 {
     if (skip(a.cond)) return;
@@ -179,17 +182,18 @@ __global__ void __launch_bounds__(256) k_cell_order(BinArgs a)
     int lo = a.cstart[c], hi = a.cstart[c + 1];
     for (int k = lo + 1; k < hi; ++k) {
         int id = a.sidx[k];
-        double2 ps = a.spos[k];
         int j = k - 1;
         while (j >= lo && a.sidx[j] > id) {
             a.sidx[j + 1] = a.sidx[j];
-            a.spos[j + 1] = a.spos[j];
             --j;
         }
         a.sidx[j + 1] = id;
-        a.spos[j + 1] = ps;
     }
-    for (int k = lo; k < hi; ++k) a.slot_of[a.sidx[k]] = k;
+    for (int k = lo; k < hi; ++k) {
+        const int id = a.sidx[k];
+        a.slot_of[id] = k;
+        a.spos[k] = a.pos[id];
+    }
 }
 
 // current positions into cell order; largest distance outside the listing cell (index order:

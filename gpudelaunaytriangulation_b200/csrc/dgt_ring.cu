@@ -1182,8 +1182,10 @@ __device__ __forceinline__ void test_spoke(double2 prev, double2 cur, double2 nx
 // Flip mode (A.flip_list set): a valid fan (every triangle strictly CCW, winding once) sends
 // its illegal or undecided spokes (i, P_k) with i < P_k to the flip list (the flip stage
 // decides them exactly); an invalid fan queues its point for rebuilding.
+// four blocks per SM (64 registers): more warps in flight hide the neighbour gathers
+// (measured: -4% repair time against three blocks at 73 registers)
 template <bool GEN>
-__global__ void __launch_bounds__(256) k_test(TestArgs A)
+__global__ void __launch_bounds__(256, 4) k_test(TestArgs A)
 {
     unsigned long long flagged = 0;
     const int ebase = *A.epoch_ptr + 1;
