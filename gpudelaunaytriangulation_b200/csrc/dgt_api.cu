@@ -765,7 +765,8 @@ int repair_impl(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, i
             a.n_items = c->n;
             a.repair = 1;
             a.cand_by_index = 1;
-            // a round that fits one wave of the warp-per-point kernel goes there whole
+            // a round of at most 16 points per SM goes to the warp-per-point kernel whole (two
+            // points per resident warp)
             a.warp_items = c->sms * 16;
             a.epoch_ptr = &ctl->epoch;
             a.round = round;
