@@ -120,7 +120,7 @@ extern "C" int dgt_global_triangulation_noalloc(const double *d_points, int n, d
     if (a < amin) a = amin;
     int xs = std::max(1, (int)std::floor(Lx / a)), ys = std::max(1, (int)std::floor(Ly / a));
     if ((long long)xs * ys > NA_MAX_CELLS) return DGT_ERR_INVALID_ARGUMENT;
-    SetDesc S;
+    SetDesc S{};   // value-initialised: every field not set below (general box, ...) is zero
     S.Lx = Lx;
     S.Ly = Ly;
     S.hLx = 0.5 * Lx;
