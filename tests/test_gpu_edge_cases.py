@@ -94,3 +94,26 @@ def test_coordinates_on_the_box_edges():
     assert ok, rep
     ref = O.restated_global(pts, L, L, 1.0, 32)
     assert np.array_equal(O.canonical(t, k)[:, :16], O.canonical(ref.tri, ref.nn)[:, :16])
+
+
+def test_largest_single_set_and_repair():
+    # 2^24 points (4x the largest benchmark set): index arithmetic and grid sizes past 2^24
+    # cells; checked on the device (validator) and by the ring-size sum, which is 6N exactly
+    # on the torus
+    DelaunayGPU, _ = _dg()
+    n = 1 << 24
+    L = float(np.sqrt(n))
+    g = torch.Generator(device="cuda").manual_seed(77)
+    P = torch.rand((n, 2), generator=g, device="cuda", dtype=torch.float64) * L
+    d = DelaunayGPU(n, 16, 1.0, (L, L))
+    tri, nn = d.globalDelaunayTriangulation(P)
+    st = d.stats()
+    assert st["error_flags"] == 0 and st["mismatches"] == 0
+    assert int(nn.sum().item()) == 6 * n
+    assert d.validate(P, tri, nn)["valid"] == 1
+    P.add_(torch.randn((n, 2), generator=g, device="cuda", dtype=torch.float64), alpha=0.02)
+    P.remainder_(L)
+    P.masked_fill_(P >= L, 0.0)   # a tiny negative coordinate plus L rounds to L
+    d.testAndRepairDelaunayTriangulation(P, tri, nn)
+    assert d.stats()["error_flags"] == 0
+    assert d.validate(P, tri, nn)["valid"] == 1

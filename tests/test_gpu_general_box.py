@@ -197,3 +197,33 @@ def test_batch_of_general_and_rectangular_boxes_matches_single_sets():
             assert _same_rings(ts, k[lo:hi], t1, k1), (step, s)
             ok, rep = O.verify_general(sets[s], box, ts, k[lo:hi])
             assert ok, (step, s, rep)
+
+
+def test_general_box_argument_and_input_errors():
+    from gpudelaunaytriangulation_b200 import _native as N
+
+    DelaunayGPU, PeriodicBox = _dgpu()
+    n = 2000
+    box = _box_of_area(n, OBLIQUE)
+    # degenerate (parallel lattice vectors) and non-finite matrices are refused
+    for bad in [(10.0, 20.0, 5.0, 10.0), (10.0, 0.0, float("nan"), 10.0), (float("inf"), 1.0, 0.0, 10.0)]:
+        with pytest.raises(N.DgtError) as e:
+            DelaunayGPU(n, 16, 1.0, PeriodicBox.general(*bad))
+        assert e.value.code == N.DGT_ERR_INVALID_ARGUMENT
+    # a non-finite coordinate is reported, and the context stays usable
+    pts = _oblique_points(n, box, 53)
+    d = DelaunayGPU(n, 16, 1.0, box)
+    bad_pts = pts.copy()
+    bad_pts[7, 0] = float("nan")
+    with pytest.raises(N.DgtError) as e:
+        d.globalDelaunayTriangulation(torch.from_numpy(bad_pts).cuda())
+    assert e.value.code == N.DGT_ERR_BAD_POINTS
+    P = torch.from_numpy(pts).cuda()
+    tri, nn = d.globalDelaunayTriangulation(P)
+    assert d.validate(P, tri, nn)["valid"] == 1
+    # too few points to close a ring, as in a rectangular box
+    small = _box_of_area(3, HEX)
+    d3 = DelaunayGPU(3, 16, 1.0, small)
+    with pytest.raises(N.DgtError) as e:
+        d3.globalDelaunayTriangulation(torch.from_numpy(_oblique_points(3, small, 54)).cuda())
+    assert e.value.code == N.DGT_ERR_DEGENERATE
