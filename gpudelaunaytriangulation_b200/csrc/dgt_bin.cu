@@ -51,19 +51,19 @@ __global__ void __launch_bounds__(256) k_clear_counts(int *ccount, int ncell, in
 __global__ void __launch_bounds__(256) k_count(BinArgs a, DevStatus *st)
 {
     if (skip(a.cond)) return;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.n) return;
-    const SetDesc &S = a.sets[a.set_of ? a.set_of[i] : 0];
-    double2 p = a.pos[i];
-    if (bad_input(S, p)) {
-        atomicOr(&st->err_flags, EF_BAD_INPUT);
-        p = make_double2(0.0, 0.0);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        const SetDesc &S = a.sets[a.set_of ? a.set_of[i] : 0];
+        double2 p = a.pos[i];
+        if (bad_input(S, p)) {
+            atomicOr(&st->err_flags, EF_BAD_INPUT);
+            p = make_double2(0.0, 0.0);
+        }
+        int c = cell_index(S, p);
+        a.cell_of[i] = c;
+        a.rank[i] = atomicAdd(&a.ccount[c], 1);
+        int lc = c - S.cell_base, cy = lc / S.xsize, cx = lc - cy * S.xsize;
+        atomicAdd(&a.bcount[S.block_base + (cy >> BLOCK_SHIFT) * S.bxsize + (cx >> BLOCK_SHIFT)], 1);
     }
-    int c = cell_index(S, p);
-    a.cell_of[i] = c;
-    a.rank[i] = atomicAdd(&a.ccount[c], 1);
-    int lc = c - S.cell_base, cy = lc / S.xsize, cx = lc - cy * S.xsize;
-    atomicAdd(&a.bcount[S.block_base + (cy >> BLOCK_SHIFT) * S.bxsize + (cx >> BLOCK_SHIFT)], 1);
 }
 
 constexpr int SCAN_THREADS = 1024;
@@ -162,13 +162,13 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(const int *in, int 
 __global__ void __launch_bounds__(256) k_scatter(BinArgs a)
 {
     if (skip(a.cond)) return;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.n) return;
-    int slot = a.cstart[a.cell_of[i]] + a.rank[i];
-    a.sidx[slot] = i;
-    if (!a.deterministic) {
-        a.spos[slot] = a.pos[i];
-        a.slot_of[i] = slot;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        int slot = a.cstart[a.cell_of[i]] + a.rank[i];
+        a.sidx[slot] = i;
+        if (!a.deterministic) {
+            a.spos[slot] = a.pos[i];
+            a.slot_of[i] = slot;
+        }
     }
 }
 
@@ -177,22 +177,22 @@ __global__ void __launch_bounds__(256) k_scatter(BinArgs a)
 __global__ void __launch_bounds__(256) k_cell_order(BinArgs a)
 {
     if (skip(a.cond)) return;
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= a.total_cells) return;
-    int lo = a.cstart[c], hi = a.cstart[c + 1];
-    for (int k = lo + 1; k < hi; ++k) {
-        int id = a.sidx[k];
-        int j = k - 1;
-        while (j >= lo && a.sidx[j] > id) {
-            a.sidx[j + 1] = a.sidx[j];
-            --j;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < a.total_cells; c += gridDim.x * blockDim.x) {
+        int lo = a.cstart[c], hi = a.cstart[c + 1];
+        for (int k = lo + 1; k < hi; ++k) {
+            int id = a.sidx[k];
+            int j = k - 1;
+            while (j >= lo && a.sidx[j] > id) {
+                a.sidx[j + 1] = a.sidx[j];
+                --j;
+            }
+            a.sidx[j + 1] = id;
         }
-        a.sidx[j + 1] = id;
-    }
-    for (int k = lo; k < hi; ++k) {
-        const int id = a.sidx[k];
-        a.slot_of[id] = k;
-        a.spos[k] = a.pos[id];
+        for (int k = lo; k < hi; ++k) {
+            const int id = a.sidx[k];
+            a.slot_of[id] = k;
+            a.spos[k] = a.pos[id];
+        }
     }
 }
 
@@ -241,14 +241,23 @@ cudaError_t launch_scan(const int *in, int n, int *bsum, int *out, cudaStream_t 
 
 int scan_block_count(int n) { return (n + SCAN_TILE - 1) / SCAN_TILE; }
 
+// One thread per item; a binning that may be skipped on the device (a.cond) runs a capped,
+// grid-stride grid instead, so a skipped launch costs a few microseconds, not one block per
+// 256 items
+static int bin_grid(int items, const int *cond)
+{
+    const int full = (items + 255) / 256;
+    return cond ? (full < 1024 ? full : 1024) : full;
+}
+
 // BinArgs.ccount must hold total_cells + 1 zeros when this is called (the API clears it)
 cudaError_t launch_bin_st(const BinArgs &a, DevStatus *st, cudaStream_t s)
 {
-    if (a.n > 0) k_count<<<(a.n + 255) / 256, 256, 0, s>>>(a, st);
+    if (a.n > 0) k_count<<<bin_grid(a.n, a.cond), 256, 0, s>>>(a, st);
     cudaError_t e = launch_scan_c(a.ccount, a.total_cells + 1, a.block_sums, a.cstart, a.cond, s);
     if (e != cudaSuccess) return e;
-    if (a.n > 0) k_scatter<<<(a.n + 255) / 256, 256, 0, s>>>(a);
-    if (a.deterministic && a.total_cells > 0) k_cell_order<<<(a.total_cells + 255) / 256, 256, 0, s>>>(a);
+    if (a.n > 0) k_scatter<<<bin_grid(a.n, a.cond), 256, 0, s>>>(a);
+    if (a.deterministic && a.total_cells > 0) k_cell_order<<<bin_grid(a.total_cells, a.cond), 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -269,7 +278,7 @@ cudaError_t launch_clear_counts(int *ccount, int ncell, int *bcount, int nblock,
 {
     const int m = ncell > nblock ? ncell : nblock;
     int blocks = (m + 255) / 256;
-    if (blocks > 4096) blocks = 4096;
+    if (blocks > (cond ? 1024 : 4096)) blocks = cond ? 1024 : 4096;
     if (blocks < 1) blocks = 1;
     k_clear_counts<<<blocks, 256, 0, s>>>(ccount, ncell, bcount, nblock, cond);
     return cudaGetLastError();
