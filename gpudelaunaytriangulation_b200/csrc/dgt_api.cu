@@ -755,6 +755,11 @@ int repair_impl(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, i
         DGT_TRY(launch_bin_st(a, dst, s));
         c->launches += 2 + (c->n > 0 ? 2 : 0) + 3 + (c->deterministic && c->total_cells > 0 ? 1 : 0);
     }
+    if (c->flip) {
+        c->launches += 1;
+        DGT_TRY(launch_expand(lists[0], &dst->list_count[0], c->n, d_tri, d_nn, stride, c->n, c->mark.as<int>(),
+                              &ctl->epoch, c->sms, s));
+    }
     int round = 0;
     bool pending = false;
     for (;;) {

@@ -314,5 +314,8 @@ cudaError_t launch_displace(double2 *pos, int n, const SetDesc *sets, const int 
 // end of a test-and-repair call: fold flags into the sticky word, check convergence,
 // advance the epoch by rounds + 1
 cudaError_t launch_call_end(DevCtl *ctl, DevStatus *st, int rounds, cudaStream_t s);
+// first rebuild round of a flip-mode repair: the current ring neighbours of its points join it
+cudaError_t launch_expand(int *list, int *count, int cap, const int *tri, const int *nn, int stride, int n,
+                          int *mark, const int *epoch_ptr, int sms, cudaStream_t s);
 
 }  // namespace dgt

@@ -1357,6 +1357,42 @@ cudaError_t launch_test(const TestArgs &a, cudaStream_t s)
     return cudaGetLastError();
 }
 
+// The points of the first rebuild round take their current ring neighbours along: a rebuilt
+// point's old and new neighbours are what the consistency checks would queue for the next
+// round, and a round costs about the same for a few points as for a wave of them.  Only a
+// list of at most max_items / 8 points is expanded (the result stays within one wave).
+__global__ void __launch_bounds__(256) k_expand(int *list, int *count, int cap, const int *tri, const int *nn,
+                                                int stride, int n, int *mark, const int *epoch_ptr, int max_items)
+{
+    const int ebase = *epoch_ptr + 1;
+    const int n0 = min(*count, cap);
+    if (n0 > max_items / 8) return;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n0; t += gridDim.x * blockDim.x) {
+        const int i = list[t];
+        if (i < 0 || i >= n) continue;
+        const int m = nn[i];
+        if (m < 1 || m > stride) continue;
+        const int *row = tri + (size_t)i * stride;
+        for (int k = 0; k < m; ++k) {
+            const int j = row[k];
+            if (j < 0 || j >= n) continue;
+            if (atomicMax(&mark[j], ebase) < ebase) {
+                const int at = atomicAdd(count, 1);
+                if (at < cap) list[at] = j;
+            }
+        }
+    }
+}
+
+cudaError_t launch_expand(int *list, int *count, int cap, const int *tri, const int *nn, int stride, int n,
+                          int *mark, const int *epoch_ptr, int sms, cudaStream_t s)
+{
+    // one wave of the per-thread rebuild kernel: 8 blocks of 64 threads per SM
+    k_expand<<<max(sms, 1) * 4, 256, 0, s>>>(list, count, cap, tri, nn, stride, n, mark, epoch_ptr,
+                                             max(sms, 1) * 8 * 64);
+    return cudaGetLastError();
+}
+
 __global__ void k_call_end(DevCtl *ctl, DevStatus *st, int rounds)
 {
     int f = st->err_flags;
