@@ -227,3 +227,17 @@ def test_general_box_argument_and_input_errors():
     with pytest.raises(N.DgtError) as e:
         d3.globalDelaunayTriangulation(torch.from_numpy(_oblique_points(3, small, 54)).cuda())
     assert e.value.code == N.DGT_ERR_DEGENERATE
+
+
+def test_kernel_box_is_the_oracle_reduction():
+    DelaunayGPU, PeriodicBox = _dgpu()
+    rng = np.random.default_rng(55)
+    for _ in range(20):
+        a = rng.uniform(-30, 30, 2)
+        b = rng.uniform(-30, 30, 2)
+        box = (a[0], b[0], a[1], b[1])
+        if abs(a[0] * b[1] - a[1] * b[0]) < 50.0 or (box[1] == 0.0 and box[2] == 0.0):
+            continue
+        d = DelaunayGPU(100, 16, 1.0, PeriodicBox.general(*box))
+        assert d.kernelBox() == O.reduce_basis(box)
+        d.close()

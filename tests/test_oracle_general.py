@@ -7,6 +7,7 @@ must keep the triangulation."""
 from fractions import Fraction as F
 
 import numpy as np
+import pytest
 
 from gpudelaunaytriangulation_b200 import workloads as W
 from oracle import oracle as O
@@ -113,3 +114,23 @@ def test_verifier_general_box_invariances_and_planted_faults():
     moved[30] += 0.3
     ok, rep = O.verify_general(moved, rbox, t.tri, t.nn)
     assert not ok and (rep["not_local_dt"] > 0 or rep["nonpositive"] > 0)
+
+
+def test_python_box_mirror_wraps_into_the_unit_cell():
+    # PeriodicBox (the host mirror of periodicBoundaries) on the CPU: the same box from a
+    # tuple, the reference's getBoxDims order, and putInBoxReal for a general box keeping
+    # each point's lattice class
+    torch = pytest.importorskip("torch")
+    from gpudelaunaytriangulation_b200.delaunay import PeriodicBox
+
+    b = PeriodicBox.of((10.0, 4.0, 1.0, 8.0))
+    assert not b.isBoxSquare() and b.getBoxDims() == (10.0, 4.0, 1.0, 8.0)
+    assert PeriodicBox.of((5.0, 6.0)).isBoxSquare()
+    rng = np.random.default_rng(14)
+    p = torch.from_numpy(rng.uniform(-40.0, 40.0, (500, 2)))
+    q = b.putInBoxReal(p).numpy()
+    M = np.array([[10.0, 4.0], [1.0, 8.0]])
+    u = q @ np.linalg.inv(M).T
+    assert np.all(u >= -1e-12) and np.all(u < 1.0 + 1e-12)
+    shift = (p.numpy() - q) @ np.linalg.inv(M).T
+    assert np.allclose(shift, np.round(shift), atol=1e-9)
