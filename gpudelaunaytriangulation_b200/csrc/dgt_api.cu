@@ -61,7 +61,7 @@ constexpr int FLIP_BATCH = 4;       // flip rounds launched before each host che
 // points, sigma 0.02: repair 1.64 -> 1.49 ms against flipping to the end)
 constexpr int SPILL_EDGES_PER_SM = 64;
 constexpr int MAX_FLIP_ROUNDS = 24; // flip rounds of a checked call before the rest is rebuilt
-constexpr int ASYNC_FLIP_ROUNDS = 3; // flip rounds of an unsynchronised call (measured best of 1-10 for MD steps)
+constexpr int ASYNC_FLIP_ROUNDS = 3; // default flip rounds of an unsynchronised call (best of 1-10 for MD steps at sigma 0.01)
 
 }  // namespace
 
@@ -99,6 +99,7 @@ struct dgt_context {
     int shape = 0;   // kernel shape (ring capacity, block size), see dgt_set_kernel_shape
     int work_budget = DEFAULT_WORK_BUDGET;   // per-point cells + candidates of the per-thread kernel
     int flip = 1;    // test-and-repair starts with edge flips (0: rebuild every flagged point)
+    int graph_flip_rounds = ASYNC_FLIP_ROUNDS;   // flip rounds of unsynchronised calls
     bool binned = false;   // the cell lists hold a binning of the current grid
     int flip_cap = 0;
 };
@@ -724,7 +725,7 @@ int repair_impl(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, i
         f.st = dst;
         int fr = 0;
         for (;;) {
-            const int batch = fixed_rounds > 0 ? ASYNC_FLIP_ROUNDS : FLIP_BATCH;
+            const int batch = fixed_rounds > 0 ? c->graph_flip_rounds : FLIP_BATCH;
             for (int b = 0; b < batch; ++b, ++fr) {
                 f.cur = flips[fr & 1];
                 f.cur_count = &dst->flip_count[fr & 1];
@@ -1088,6 +1089,13 @@ int dgt_get_cell_order(dgt_context *c, int *d_order, void *stream)
     if (!d_order || !c->binned) return DGT_ERR_INVALID_ARGUMENT;
     DGT_TRY(cudaMemcpyAsync(d_order, c->sidx.p, sizeof(int) * (size_t)c->n, cudaMemcpyDeviceToDevice,
                             (cudaStream_t)stream));
+    return DGT_OK;
+}
+
+int dgt_set_graph_flip_rounds(dgt_context *c, int rounds)
+{
+    if (!c || rounds < 0 || rounds > MAX_FLIP_ROUNDS) return DGT_ERR_INVALID_ARGUMENT;
+    c->graph_flip_rounds = rounds;
     return DGT_OK;
 }
 

@@ -325,6 +325,11 @@ class DelaunayGPU:
         """Test-and-repair by Lawson flips first (default) or by rebuilding every flagged point."""
         _nat.check(self._L.dgt_set_flip_repair(self._h, int(bool(on))), "dgt_set_flip_repair")
 
+    def setGraphFlipRounds(self, rounds: int):
+        """Flip rounds of mdStep / mdGraph repairs (0..24, default 3; more pay off for larger
+        displacements).  A graph keeps the value it was captured with."""
+        _nat.check(self._L.dgt_set_graph_flip_rounds(self._h, int(rounds)), "dgt_set_graph_flip_rounds")
+
     def setWorkBudget(self, budget: int):
         """Cells + candidates a point may scan in the thread-per-point kernel before the
         warp-per-point kernel takes it over (0: every point goes to the warp kernel)."""

@@ -56,6 +56,7 @@ def test_invalid_arguments_without_device():
     assert L.dgt_get_max_size(None, ctypes.byref(v)) == N.DGT_ERR_INVALID_ARGUMENT
     assert L.dgt_restride(None, 4, None, 8, None, 5, None) == N.DGT_ERR_INVALID_ARGUMENT
     assert L.dgt_set_box_general(None, 1.0, 0.5, 0.0, 1.0) == N.DGT_ERR_INVALID_ARGUMENT
+    assert L.dgt_set_graph_flip_rounds(None, 3) == N.DGT_ERR_INVALID_ARGUMENT
     box = (ctypes.c_double * 4)()
     assert L.dgt_get_box(None, box) == N.DGT_ERR_INVALID_ARGUMENT
     L.dgt_destroy(None)

@@ -47,6 +47,18 @@ def test_md_steps_without_graph():
     check_sets(P, tri, nn, sizes, boxes)
 
 
+@pytest.mark.parametrize("flip_rounds", [0, 6])
+def test_md_steps_with_other_flip_round_counts(flip_rounds):
+    # every flagged edge rebuilt (0 flip rounds) or flipped longer (6): same triangulation
+    b, P, tri, nn, sizes, boxes = setup(seed=22)
+    b.setGraphFlipRounds(flip_rounds)
+    for _ in range(3):
+        b.mdStep(P, tri, nn, 0.03, seed=6, rounds=6)
+    torch.cuda.synchronize()
+    assert b.stats()["sticky_flags"] == 0
+    check_sets(P, tri, nn, sizes, boxes)
+
+
 def test_md_graph_replays_fresh_noise_and_matches_oracle():
     b, P, tri, nn, sizes, boxes = setup(seed=22)
     stream = torch.cuda.Stream()
