@@ -61,7 +61,7 @@ constexpr int FLIP_BATCH = 4;       // flip rounds launched before each host che
 // points, sigma 0.02: repair 1.64 -> 1.49 ms against flipping to the end)
 constexpr int SPILL_EDGES_PER_SM = 64;
 constexpr int MAX_FLIP_ROUNDS = 24; // flip rounds of a checked call before the rest is rebuilt
-constexpr int ASYNC_FLIP_ROUNDS = 3; // default flip rounds of an unsynchronised call (best for small steps; they also stop on the device once the list is short)
+constexpr int ASYNC_FLIP_ROUNDS = 3; // default flip rounds of an unsynchronised call (best of 1-10 for MD steps at sigma 0.01)
 
 }  // namespace
 
@@ -722,8 +722,6 @@ int repair_impl(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, i
         f.stamp_ptr = &ctl->flip_stamp;
         f.quad = c->quad.as<int2>();
         f.cap = c->flip_cap;
-        // unsynchronised calls stop on the device once the list is short (see the knob)
-        f.stop_below = fixed_rounds > 0 ? c->sms * SPILL_EDGES_PER_SM : 0;
         f.st = dst;
         int fr = 0;
         for (;;) {
@@ -744,8 +742,6 @@ int repair_impl(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, i
         }
         f.cur = flips[fr & 1];
         f.cur_count = &dst->flip_count[fr & 1];
-        f.next = flips[(fr + 1) & 1];
-        f.next_count = &dst->flip_count[(fr + 1) & 1];
         c->launches += 2;
         DGT_TRY(launch_flip_spill(f, fr, ctl, c->sms, s));
     }

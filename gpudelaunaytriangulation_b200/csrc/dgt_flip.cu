@@ -130,25 +130,12 @@ __device__ __forceinline__ unsigned long long claim_key(unsigned stamp, int slot
     return ((unsigned long long)stamp << 32) | x;
 }
 
-// Early stop of an unsynchronised repair's flips (FlipArgs::stop_below): every thread of a
-// round decides alike from the list length (a thread of the stopping round that already
-// sees the flag returns as well); the stopping round records itself, and later rounds,
-// launched after it completed, return on the flag before touching any list
-__device__ __forceinline__ bool flips_stopped(const FlipArgs &A, int round, int n)
-{
-    if (A.st->flip_stopped) return true;
-    if (A.stop_below <= 0 || round == 0 || n > A.stop_below) return false;
-    if (blockIdx.x == 0 && threadIdx.x == 0) A.st->flip_stopped = round + 1;
-    return true;
-}
-
 template <bool GEN>
 __global__ void __launch_bounds__(256, 2) k_flip_claim(FlipArgs A, int round)
 {
     const int ebase = *A.epoch_ptr + 1;
     const unsigned stamp = *A.stamp_ptr + 1 + round;
     const int n = min(*A.cur_count, A.cap);
-    if (flips_stopped(A, round, n)) return;
     // the next round's list is appended by this round's apply kernel: cleared here (the last
     // reader of that buffer, the previous round's apply, has finished) instead of by a memset
     if (blockIdx.x == 0 && threadIdx.x == 0) *A.next_count = 0;
@@ -217,7 +204,6 @@ __global__ void __launch_bounds__(256, 2) k_flip_apply(FlipArgs A, int round)
     const int ebase = *A.epoch_ptr + 1;
     const unsigned stamp = *A.stamp_ptr + 1 + round;
     const int n = min(*A.cur_count, A.cap);
-    if (A.st->flip_stopped) return;   // set by this round's claim kernel or an earlier round
     unsigned long long flips = 0;
     // warp-uniform trip count: every lane reaches the warp-aggregated append
     for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
@@ -288,19 +274,14 @@ __global__ void __launch_bounds__(256, 2) k_flip_apply(FlipArgs A, int round)
 __global__ void __launch_bounds__(256) k_flip_spill(FlipArgs A, int rounds)
 {
     const int ebase = *A.epoch_ptr + 1;
-    // the list left: that of the round that stopped early, else that after the last round
-    // (A.cur); with two alternating lists, the other one is A.next
-    const int stopped = A.st->flip_stopped;
-    const bool other = stopped > 0 && ((stopped - 1) & 1) != (rounds & 1);
-    const int2 *list = other ? A.next : A.cur;
-    const int n = min(other ? *A.next_count : *A.cur_count, A.cap);
+    const int n = min(*A.cur_count, A.cap);
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
-        const int2 ed = list[e];
+        const int2 ed = A.cur[e];
         to_rebuild(A, ebase, ed.x);
         to_rebuild(A, ebase, ed.y);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        atomicMax(&A.st->flip_rounds, stopped > 0 ? stopped - 1 : rounds);
+        atomicMax(&A.st->flip_rounds, rounds);
         if (n > 0) atomicAdd(&A.st->flip_spilled, (unsigned long long)n);
     }
 }

@@ -137,8 +137,6 @@ struct DevStatus {
     unsigned long long flips;           // test-and-repair: edge flips applied
     unsigned long long flip_spilled;    // flip candidates left after the last flip round
     int flip_rounds;                    // flip rounds run
-    int flip_stopped;                   // unsynchronised repair: 1 + the round that stopped the flips early
-                                        // (0: none); its list (round & 1) holds what is left
     int rebin;                          // repair: 1 when this call rebuilt the cell lists
     float skin_measured;                // repair: largest move since binning, in cells (per axis)
     float skin;                         // certification margin of this call's rebuilds, in cells
@@ -275,10 +273,6 @@ struct FlipArgs {
     int2 *next;                 // candidates of the next round
     int *next_count;
     int cap;                    // capacity of cur / next / quad
-    // unsynchronised repairs: a round (after the first) whose list holds at most this many
-    // candidates stops the flips -- it and every later round return at once and the spill
-    // takes its list to the rebuild rounds (0: never)
-    int stop_below;
     int general = 0;            // 1: general-box instantiations (SetDesc::general)
     DevStatus *st;
 };

@@ -239,10 +239,9 @@ int dgt_set_work_budget(dgt_context *ctx, int budget);
  * and the four points of every failing spoke, as the reference does.  Same result. */
 int dgt_set_flip_repair(dgt_context *ctx, int on);
 /* Flip rounds of the unsynchronised repair calls (dgt_md_step, and dgt_md_graph_create at
- * capture time; no reference counterpart): 0..24, default 3.  The rounds stop early on the
- * device once at most 64 candidates per SM are left; what the flips leave goes to the
- * rebuild rounds.  Measured on 256 sets / 3.98M points per MD step at sigma 0.01 / 0.02 /
- * 0.05: 3 rounds 1.02 / 1.46 / 3.62 ms, 8 rounds 1.17 / 1.44 / 2.88 ms -- raise it for
+ * capture time; no reference counterpart): 0..24, default 3.  What the flips leave goes to
+ * the rebuild rounds.  Measured on 256 sets / 3.98M points per MD step at sigma 0.01 / 0.02
+ * / 0.05: 3 rounds 1.02 / 1.46 / 3.62 ms, 6 rounds 1.06 / 1.47 / 2.86 ms -- raise it for
  * larger displacements.  Synchronised calls decide on the host instead. */
 int dgt_set_graph_flip_rounds(dgt_context *ctx, int rounds);
 int dgt_get_tuning(const dgt_context *ctx, double *cell_size, int *shape, int *ring_capacity, int *block);
