@@ -188,6 +188,11 @@ class DelaunayGPU {
     void setOMPthreads(unsigned int) {}
     void setPrecision(int precision) { check(dgt_set_precision(ctx_, precision), "setPrecision"); }
     void setStream(cudaStream_t s) { stream_ = s; }
+    // knobs without a reference counterpart (include/dgt.h); none changes the output
+    void setFlipRepair(bool on) { check(dgt_set_flip_repair(ctx_, on ? 1 : 0), "setFlipRepair"); }
+    void setWorkBudget(int budget) { check(dgt_set_work_budget(ctx_, budget), "setWorkBudget"); }
+    void setGraphFlipRounds(int rounds) { check(dgt_set_graph_flip_rounds(ctx_, rounds), "setGraphFlipRounds"); }
+    void setCheckMode(bool on) { check(dgt_set_check_mode(ctx_, on ? 1 : 0), "setCheckMode"); }
     int MaxSize() const
     {
         int v = 0;
