@@ -10,20 +10,27 @@
 //
 // Limits: at most DGT_NOALLOC_MAX_POINTS points and DGT_NOALLOC_MAX_CELLS grid cells; larger
 // inputs are rejected with DGT_ERR_INVALID_ARGUMENT before any work is queued.  The array
-// (about 4.8 MB) exists on every GPU that loads this library, until the process exits.
+// (NA_BYTES = 4,720,384 bytes, about 4.72 MB) exists on every GPU that loads this library,
+// until the process exits.
 //
 // Sharing: all calls use the same array and it keeps the last call's contents; the parts
 // that must start at zero (cell counts, status block) are cleared by every call.  Calls
 // whose kernels overlap on a GPU (different streams or host threads without ordering)
 // race on the array; callers must order them.
 //
-// Set-up: the first call on a device, with that device current, looks the array's
-// device address up once (cudaGetSymbolAddress; host code cannot use the array's name as a
-// device pointer) and caches it per device.  Make that first call before any stream capture.
+// Set-up: every call, with the caller's device current, looks up the array's device address
+// (cudaGetSymbolAddress; in host code the array's name is only a host-side stand-in, never a
+// device address).  Nothing is cached: after a cudaDeviceReset, or in another context on the
+// same device, the library's module is loaded again at another address, and a cached pointer
+// would send the kernels to stale memory.  The lookup is a host-side call, small next to the
+// synchronisation that ends every call.
+//
+// Synchronisation: a call copies its status to pageable host memory and synchronises
+// `stream`, so it must not be called while `stream` (or any stream in global capture mode) is
+// capturing a CUDA graph.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
-#include <mutex>
 
 #include "dgt.h"
 #include "dgt_internal.cuh"
@@ -62,22 +69,13 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
 
 namespace {
 
-constexpr int NA_MAX_DEVICES = 64;
-unsigned char *g_base[NA_MAX_DEVICES] = {};
-std::mutex g_setup_mutex;
-
-// once per device, with that device current: the array's device address
-int scratch_base(int dev, unsigned char **out)
+// the array's device address in the current context (looked up on every call, see above)
+int scratch_base(unsigned char **out)
 {
-    if (dev < 0 || dev >= NA_MAX_DEVICES) return DGT_ERR_INVALID_ARGUMENT;
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_base[dev]) {
-        void *ptr = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-        if (e != cudaSuccess || !ptr) return DGT_ERR_CUDA;
-        g_base[dev] = static_cast<unsigned char *>(ptr);
-    }
-    *out = g_base[dev];
+    void *ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || !ptr) return DGT_ERR_CUDA;
+    *out = static_cast<unsigned char *>(ptr);
     return DGT_OK;
 }
 
@@ -113,12 +111,18 @@ extern "C" int dgt_global_triangulation_noalloc(const double *d_points, int n, d
     if (n == 0) return DGT_OK;
     if (n > NA_MAX_POINTS || !d_points || !d_tri || !d_neighnum || stride < 3 || stride > (1 << 16))
         return DGT_ERR_INVALID_ARGUMENT;
-    // cell grid (same rule as a context: requested edge, no finer than ~4 cells per point)
+    // cell grid: the requested edge (mean spacing when cell_size <= 0), but no finer than ~4
+    // cells per point, because the array holds a fixed number of cells (a context allows ~16);
+    // the output does not depend on the cell size
     double spacing = std::sqrt(Lx * Ly / n);
     double a = cell_size > 0 ? cell_size : spacing;
-    double amin = std::sqrt(Lx * Ly / (4.0 * n + 16.0));   // at most ~4 cells per point here
+    double amin = std::sqrt(Lx * Ly / (4.0 * n + 16.0));
     if (a < amin) a = amin;
-    int xs = std::max(1, (int)std::floor(Lx / a)), ys = std::max(1, (int)std::floor(Ly / a));
+    // judged in double before the conversion to int: a box of extreme aspect ratio can ask
+    // for more cells along one axis than an int holds
+    const double fxs = std::floor(Lx / a), fys = std::floor(Ly / a);
+    if (!(fxs <= (double)NA_MAX_CELLS) || !(fys <= (double)NA_MAX_CELLS)) return DGT_ERR_INVALID_ARGUMENT;
+    int xs = std::max(1, (int)fxs), ys = std::max(1, (int)fys);
     if ((long long)xs * ys > NA_MAX_CELLS) return DGT_ERR_INVALID_ARGUMENT;
     SetDesc S{};   // value-initialised: every field not set below (general box, ...) is zero
     S.Lx = Lx;
@@ -142,7 +146,7 @@ extern "C" int dgt_global_triangulation_noalloc(const double *d_points, int n, d
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return DGT_ERR_CUDA;
     unsigned char *base = nullptr;
-    int rc = scratch_base(dev, &base);
+    int rc = scratch_base(&base);
     if (rc != DGT_OK) return rc;
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
