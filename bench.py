@@ -49,10 +49,10 @@ WORKLOADS = {
 # counted.
 BUILD_BYTES_PER_POINT = 16 + 4 + 4 + 24 + 4
 # DRAM bytes per point that ncu measured for k_build (dram__bytes_read.sum +
-# dram__bytes_write.sum of one launch / points) on a 1,048,576-point capture
-# (profiles/k_build_fp32_1m.md); traffic scales with the number of points at fixed density,
-# so the 4M launch is reported as this figure times its points.
-BUILD_DRAM_BYTES_PER_POINT_NCU = 88.0
+# dram__bytes_write.sum of one launch / points) on a 1,048,576-point capture of the same
+# kernel (the --profile build case below); traffic scales with the number of points at fixed
+# density, so the 4M launch is reported as this figure times its points.
+BUILD_DRAM_BYTES_PER_POINT_NCU = 87.2
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -197,6 +197,53 @@ def _reference_cpu_run(n, L, sigma, cell, maxn, steps, warmup, seed, threads=Non
     if cls is not None:
         cls.close()
     return {"seconds": times, "kind": kind, "threads": threads}
+
+
+def reference_gpu_run(n, L, sigma, cell, p0, p1, steps, warmup, ours=None):
+    """The reference's own CUDA kernels (its DelaunayGPU class with GPUcompute=true and safety
+    mode, compiled for sm_100a into oracle/_ref) on the same workload: per step a global
+    triangulation of p0 and a test-and-repair with p1, each timed with CUDA events on the
+    legacy default stream it launches on.  maxNeighs 24: its seed pass has no row-capacity
+    check, and its largest seed polygon on this workload (measured on the host first, below)
+    must stay well inside the rows.  ours: (tri, nn) of this library for p0 and for p1, to
+    count the rings that differ."""
+    from oracle import oracle as O
+
+    with _StdoutToStderr():
+        seed_max = max(O.reference_seed_max(p0, L, L, cell, 64), O.reference_seed_max(p1, L, L, cell, 64))
+        if not (0 < seed_max <= 12):
+            return {"unavailable": f"seed polygons of {seed_max} entries: too close to the 24-entry rows"}
+        R = O.ReferenceGPU(p0, p1, L, L, 24, cell)
+        diff = {}
+        for it in range(warmup):
+            R.build()
+            if not R.triangles_ok():
+                R.close()
+                return {"unavailable": "its build is not a 2N-triangle torus triangulation; repair not run"}
+            if it == 0 and ours is not None:
+                diff["build"] = _rings_differing(R.fetch(32), *ours[0])
+            R.repair()
+            if it == 0 and ours is not None:
+                diff["repair"] = _rings_differing(R.fetch(32), *ours[1])
+        b_ms, r_ms = [], []
+        for _ in range(steps):
+            b_ms.append(R.build())
+            r_ms.append(R.repair())   # refuses (raises) unless the build has exactly 2N triangles
+        R.close()
+    step = float(np.mean(b_ms) + np.mean(r_ms))
+    return {"value": n / step / 1e3, "unit": UNIT, "ms_per_step": step, "build_ms": float(np.mean(b_ms)),
+            "repair_ms": float(np.mean(r_ms)), "steps": steps, "max_neighs": 24, "seed_polygon_max": seed_max,
+            "rings_differing_from_ours": diff,
+            "path": "reference DelaunayGPU class, GPUcompute=true, safety mode, its CUDA kernels for sm_100a"}
+
+
+def _rings_differing(ref, tri, nn):
+    from oracle import oracle as O
+
+    if not np.array_equal(ref.nn, nn):
+        return int((ref.nn != nn).sum())
+    w = min(ref.tri.shape[1], tri.shape[1])
+    return int((O.canonical(ref.tri, ref.nn)[:, :w] != O.canonical(tri, nn)[:, :w]).any(axis=1).sum())
 
 
 def run_reference(args):
@@ -573,6 +620,19 @@ def run_ours(args):
     achieved = bytes_launch / avg_build_s / 1e9
     traffic = None if BUILD_DRAM_BYTES_PER_POINT_NCU is None else BUILD_DRAM_BYTES_PER_POINT_NCU * n
 
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_reference_gpu:
+        # this library's rings for both inputs, for the comparison (outside every timing)
+        d.setPrecision(True)
+        d.globalDelaunayTriangulation(P0, tri, nn)
+        ours0 = (tri.view(n, -1).cpu().numpy(), nn.cpu().numpy())
+        d.testAndRepairDelaunayTriangulation(P1, tri, nn)
+        ours1 = (tri.view(n, -1).cpu().numpy(), nn.cpu().numpy())
+        try:
+            ref_gpu = reference_gpu_run(n, L, sigma, cell, p0, p1, steps=3, warmup=1, ours=(ours0, ours1))
+        except Exception as e:   # reported, never fatal for this arm
+            ref_gpu = {"unavailable": f"{type(e).__name__}: {e}"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = reference_cpu_run(n, L, sigma, cell, maxn, steps=1, warmup=0, seed=seed, budget_s=30)
@@ -593,6 +653,7 @@ def run_ours(args):
                      "bytes_per_point": BUILD_BYTES_PER_POINT, "avg_launch_ms": avg_build_s * 1e3,
                      "peak_source": f"{peak_kind} hbm_gbs"},
         "cpu_baseline": cpu,
+        "reference_gpu": ref_gpu,
         "e2e": e2e,
         "gpu_launches": launches,
         "clocks": clocks,
@@ -616,6 +677,46 @@ def run_ours(args):
     return 0
 
 
+def run_profile_case(args):
+    """A fixed, small sequence of library calls for Nsight Compute captures.  `--reps` global
+    triangulations of n seeded uniform points at unit density (build, repair), or in a
+    general 60-degree box at unit density (hex); with `repair`, one test-and-repair after a
+    sigma = 0.02 displacement.  Launch order per triangulation: 6 binning kernels, k_build,
+    k_build_warp.  Prints the counters of the calls."""
+    import math
+
+    import torch
+
+    from gpudelaunaytriangulation_b200.delaunay import DelaunayGPU
+
+    n = args.n or (1 << 20)
+    L = math.sqrt(n)
+    if args.profile == "hex":
+        s = math.sqrt(n / (math.sqrt(3.0) / 2.0))
+        box = (s, 0.5 * s, 0.0, s * math.sqrt(3.0) / 2.0)
+        M = np.array([[box[0], box[1]], [box[2], box[3]]])
+        pts = np.ascontiguousarray(np.random.default_rng(7).uniform(0.0, 1.0, (n, 2)) @ M.T)
+    else:
+        box = (L, L)
+        pts = W.uniform_points(n, L, seed=7)
+    P = torch.from_numpy(pts).cuda()
+    d = DelaunayGPU(n, 16, 1.0, box)
+    d.setTiming(True)
+    tri = torch.zeros(16 * n, dtype=torch.int32, device="cuda")
+    nn = torch.zeros(n, dtype=torch.int32, device="cuda")
+    for _ in range(args.reps):
+        d.globalDelaunayTriangulation(P, tri, nn)
+    out = {"build": d.stats(), "build_ms": d.phaseTimes()}
+    if args.profile == "repair":
+        P1 = torch.from_numpy(W.displace(pts, 0.02, L, L, seed=8)).cuda()
+        d.testAndRepairDelaunayTriangulation(P1, tri, nn)
+        out["repair"] = d.stats()
+        out["repair_ms"] = d.phaseTimes()
+    torch.cuda.synchronize()
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -628,7 +729,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble MD measurement")
     ap.add_argument("--no-configs", action="store_true", help="skip the other workload families")
+    ap.add_argument("--no-reference-gpu", action="store_true", help="skip timing the reference's own CUDA kernels")
+    ap.add_argument("--profile", choices=["build", "repair", "hex"], default=None,
+                    help="profiling case for Nsight Compute: a fixed, small sequence of calls (no timing)")
+    ap.add_argument("--reps", type=int, default=2, help="global triangulations per --profile run")
     args = ap.parse_args()
+    if args.profile:
+        return run_profile_case(args)
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":

@@ -265,14 +265,16 @@ int dgt_autotune(dgt_context *ctx, const double *d_points, int *d_tri, int *d_ne
 /* Global triangulation that allocates nothing.  No counterpart in the reference: it is
  * for callers that must not call cudaMalloc (a host application owns the GPU allocator,
  * or the memory budget is fixed before this library is loaded).  All scratch lives in one
- * fixed device array inside the library (about 4.6 MB, present on every GPU that loads the
- * library until the process exits), so inputs are limited to DGT_NOALLOC_MAX_POINTS points
- * and a cell grid of DGT_NOALLOC_MAX_CELLS cells (DGT_ERR_INVALID_ARGUMENT beyond that).
- * Output and precision are those of dgt_global_triangulation (float32 filter) with safety
- * mode on: the call synchronises `stream`; on DGT_ERR_NEED_RESIZE *out_required_stride
- * (may be NULL) receives the row stride needed.  All calls share the array: calls whose
- * work overlaps on a GPU race and must be ordered by the caller.  The first call on each
- * device looks the array's address up; make it before any stream capture. */
+ * fixed device array inside the library (4,720,384 bytes, about 4.72 MB, present on every
+ * GPU that loads the library until the process exits), so inputs are limited to
+ * DGT_NOALLOC_MAX_POINTS points and a cell grid of DGT_NOALLOC_MAX_CELLS cells
+ * (DGT_ERR_INVALID_ARGUMENT beyond that, with nothing written).  Output and precision are
+ * those of dgt_global_triangulation (float32 filter) with safety mode on; on
+ * DGT_ERR_NEED_RESIZE *out_required_stride (may be NULL) receives the row stride needed.
+ * Every call looks up the array's device address in the current context, copies its status
+ * to pageable host memory and synchronises `stream`: it must not be called while a stream
+ * is capturing a CUDA graph.  All calls share the array: calls whose work overlaps on a GPU
+ * race and must be ordered by the caller. */
 #define DGT_NOALLOC_MAX_POINTS 65536
 #define DGT_NOALLOC_MAX_CELLS (4 * DGT_NOALLOC_MAX_POINTS + 16)
 int dgt_global_triangulation_noalloc(const double *d_points, int n, double Lx, double Ly, double cell_size,

@@ -9,9 +9,11 @@
 # The reference's CMake build is not used (it pins gcc-6 and sm_35, CMakeLists.txt:2-18);
 # -DNVCC is needed so HOSTDEVICE keeps __device__ (src/utilities/indexer.h:20-24) and the
 # nvtx3 include dir because inc/std_include.h:41 includes nvToolsExt.h.
+# The reference's sources: $DGT_REFERENCE_DIR, else a checkout named "reference" beside this
+# repository.
 set -euo pipefail
-REF="${DGT_REFERENCE_DIR:-/root/reference}"
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+REF="${DGT_REFERENCE_DIR:-$(dirname "$(dirname "$HERE")")/reference}"
 OUT="$HERE/_ref"
 if [ ! -f "$REF/src/model/DelaunayGPU.cu" ]; then
     echo "reference sources not found at $REF" >&2

@@ -21,6 +21,14 @@ from dataclasses import dataclass
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def reference_dir() -> str:
+    """The reference project's sources: $DGT_REFERENCE_DIR, else a checkout named
+    ``reference`` beside this repository."""
+    return os.environ.get("DGT_REFERENCE_DIR") or os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
+
+
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libdgtref.so")
 
@@ -57,11 +65,12 @@ def build(force: bool = False) -> str:
 
 def build_ref() -> str | None:
     """Compile oracle/_ref/libdgtref.so from the reference's sources when they are present."""
-    if not os.path.isdir(os.environ.get("DGT_REFERENCE_DIR", "/root/reference")):
+    if not os.path.isdir(os.path.join(reference_dir(), "src", "model")):
         return REF_PATH if os.path.exists(REF_PATH) else None
     harness = os.path.join(HERE, "ref_harness.cu")
     if not os.path.exists(REF_PATH) or os.path.getmtime(REF_PATH) < os.path.getmtime(harness):
-        subprocess.run(["bash", os.path.join(HERE, "build_ref.sh")], check=True, capture_output=True)
+        env = dict(os.environ, DGT_REFERENCE_DIR=reference_dir())
+        subprocess.run(["bash", os.path.join(HERE, "build_ref.sh")], check=True, capture_output=True, env=env)
     return REF_PATH
 
 
@@ -126,6 +135,23 @@ def ref_lib():
         R.ref_cls_destroy.restype = None
         R.ref_cls_destroy.argtypes = [ctypes.c_void_p]
         R.ref_omp_max_threads.restype = ctypes.c_int
+        R.ref_fn_seed_max.restype = ctypes.c_int
+        R.ref_fn_seed_max.argtypes = [_P_D, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_int, ctypes.c_int]
+        R.ref_gpu_create.restype = ctypes.c_void_p
+        R.ref_gpu_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_double, _P_D, _P_D]
+        _P_F = ctypes.POINTER(ctypes.c_float)
+        R.ref_gpu_build.restype = ctypes.c_int
+        R.ref_gpu_build.argtypes = [ctypes.c_void_p, _P_F]
+        R.ref_gpu_repair.restype = ctypes.c_int
+        R.ref_gpu_repair.argtypes = [ctypes.c_void_p, _P_F]
+        R.ref_gpu_triangles_ok.restype = ctypes.c_int
+        R.ref_gpu_triangles_ok.argtypes = [ctypes.c_void_p]
+        R.ref_gpu_fetch.restype = ctypes.c_int
+        R.ref_gpu_fetch.argtypes = [ctypes.c_void_p, _P_I, _P_I, ctypes.c_int]
+        R.ref_gpu_destroy.restype = None
+        R.ref_gpu_destroy.argtypes = [ctypes.c_void_p]
         _ref = R
     return _ref
 
@@ -250,6 +276,69 @@ class ReferenceClass:
     def close(self):
         if self.h:
             self.R.ref_cls_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def reference_seed_max(points, Lx, Ly, cell_size=1.0, stride=64, threads=None) -> int:
+    """Largest candidate polygon of the reference's seed pass over ``points`` (run on the
+    host); -1 if it reaches ``stride``."""
+    R = ref_lib()
+    if R is None:
+        raise RuntimeError("oracle/_ref/libdgtref.so is not built")
+    pts = _prep(points)
+    return R.ref_fn_seed_max(_pd(pts), len(pts), Lx, Ly, cell_size, stride, threads or default_threads())
+
+
+class ReferenceGPU:
+    """The reference's public DelaunayGPU class on its GPU path (its own CUDA kernels,
+    setGPUcompute(true), safety mode on): a global triangulation of ``p0`` and a
+    test-and-repair with the moved points ``p1``, each timed on the device."""
+
+    def __init__(self, p0, p1, Lx, Ly, max_neighs=24, cell_size=1.0):
+        R = ref_lib()
+        if R is None:
+            raise RuntimeError("oracle/_ref/libdgtref.so is not built")
+        self.R = R
+        a, b = _prep(p0), _prep(p1)
+        self.n = len(a)
+        self.h = R.ref_gpu_create(self.n, max_neighs, cell_size, Lx, Ly, _pd(a), _pd(b))
+        if not self.h:
+            raise RuntimeError("reference DelaunayGPU (GPU path) construction failed")
+
+    def build(self) -> float:
+        ms = ctypes.c_float(0.0)
+        if self.R.ref_gpu_build(self.h, ctypes.byref(ms)) != 0:
+            raise RuntimeError("reference GPU globalDelaunayTriangulation failed")
+        return ms.value
+
+    def triangles_ok(self) -> bool:
+        return self.R.ref_gpu_triangles_ok(self.h) == 1
+
+    def repair(self) -> float:
+        ms = ctypes.c_float(0.0)
+        r = self.R.ref_gpu_repair(self.h, ctypes.byref(ms))
+        if r == -2:
+            raise RuntimeError("reference GPU repair refused: the triangulation does not have exactly 2N triangles")
+        if r != 0:
+            raise RuntimeError("reference GPU testAndRepairDelaunayTriangulation failed")
+        return ms.value
+
+    def fetch(self, stride=32) -> Triangulation:
+        tri = np.zeros((self.n, stride), np.int32)
+        nn = np.zeros(self.n, np.int32)
+        if self.R.ref_gpu_fetch(self.h, _pi(tri), _pi(nn), stride) < 0:
+            raise RuntimeError("reference GPU fetch failed")
+        return Triangulation(tri, nn, int(nn.max()))
+
+    def close(self):
+        if self.h:
+            self.R.ref_gpu_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -20,6 +20,23 @@
  *              (src/model/DelaunayGPU.h:22-58) with setGPUcompute(false) and
  *              setOMPthreads(k).  GPUArray allocates device memory, so these entry
  *              points need a CUDA device even though all arithmetic runs on the host.
+ *
+ *  ref_gpu_* : the same class with setGPUcompute(true) and setSafetyMode(true): the
+ *              reference's own CUDA kernels (DelaunayGPU.cu:649-675 seed pass, :981-1006
+ *              refine pass, :1008-1028 triangle list, :290-313 circle test, :611-640 and
+ *              :945-975 repair passes; cellListGPU.cu:20-58 binning) compiled for sm_100a,
+ *              timed with CUDA events on the legacy default stream the reference launches
+ *              on.  Two guards keep its device writes in bounds (the reference has none for
+ *              either):
+ *                - the seed pass grows a polygon without checking the row capacity
+ *                  (DelaunayGPU.cu:568-582); ref_fn_seed_max runs the same seed pass on the
+ *                  host so a caller can check, before any GPU run, that the polygons of its
+ *                  input stay far below MaxSize;
+ *                - the triangle-list kernel appends into an array of exactly 2N entries
+ *                  (DelaunayGPU.cpp:628, DelaunayGPU.cu:1021-1025); ref_gpu_triangles_ok
+ *                  counts, on the host, the triangles of the class's current triangulation
+ *                  the way DelaunayGPU::getCircumcirclesCPU does (DelaunayGPU.cpp:673-705),
+ *                  and ref_gpu_repair refuses to run unless they are exactly 2N.
  */
 #include <vector>
 #include <cstring>
@@ -235,5 +252,164 @@ void ref_cls_destroy(void *h)
 }
 
 int ref_omp_max_threads(void) { return omp_get_max_threads(); }
+
+/* The reference's seed pass alone (gpu_voronoi_calc on the host, DelaunayGPU.cu:1116-1189),
+   over all points: returns the largest candidate polygon it builds (its rows have no
+   capacity check), or -1 when that reaches `stride` (the scratch rows here are `stride`
+   wide, so a larger polygon could not be measured; one spare row at the end keeps an
+   overflow of the last point inside the allocation). */
+int ref_fn_seed_max(const double *pts, int n, double Lx, double Ly, double cell_size, int stride, int threads)
+{
+    const double2 *p = reinterpret_cast<const double2 *>(pts);
+    BucketGrid g;
+    fill_grid(g, p, n, Lx, Ly, cell_size);
+    periodicBoundaries box(Lx, Ly);
+    Index2D ci(g.xsize, g.ysize), cli(g.nmax, g.cells), ring(stride, n);
+    std::vector<double2> P((size_t)stride * (n + 1)), Q((size_t)stride * (n + 1));
+    std::vector<int> tri((size_t)stride * (n + 1)), nn(n);
+    gpu_voronoi_calc(const_cast<double2 *>(p), g.sizes.data(), g.idx.data(), tri.data(), P.data(), Q.data(),
+                     nn.data(), n, g.xsize, g.ysize, g.boxsize, box, ci, cli, ring, false, (unsigned)threads);
+    int mx = 0;
+    for (int i = 0; i < n; ++i) mx = std::max(mx, nn[i]);
+    return mx >= stride ? -1 : mx;
+}
+
+/* ---- the reference's public class on its GPU path (its own CUDA kernels) ---- */
+struct RefGpu {
+    DelaunayGPU *del = nullptr;
+    GPUArray<double2> p0, p1;
+    GPUArray<int> tri, nn;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int n = 0;
+};
+
+/* p0: the points of the global triangulation, p1: the moved points of the repair (both
+   n x (x,y) doubles, copied to the device here, outside any timing). */
+void *ref_gpu_create(int n, int max_neighs, double cell_size, double Lx, double Ly, const double *p0,
+                     const double *p1)
+{
+    try {
+        RefGpu *r = new RefGpu();
+        r->n = n;
+        PeriodicBoxPtr box = make_shared<periodicBoundaries>(Lx, Ly);
+        r->del = new DelaunayGPU(n, max_neighs, cell_size, box);
+        r->del->setGPUcompute(true);
+        r->del->setSafetyMode(true);
+        r->p0.resize(n);
+        r->p1.resize(n);
+        r->tri.resize((unsigned)(max_neighs * n));
+        r->nn.resize(n);
+        {
+            ArrayHandle<double2> h0(r->p0, access_location::host, access_mode::overwrite);
+            ArrayHandle<double2> h1(r->p1, access_location::host, access_mode::overwrite);
+            std::memcpy(h0.data, p0, sizeof(double2) * (size_t)n);
+            std::memcpy(h1.data, p1, sizeof(double2) * (size_t)n);
+        }
+        {   // resident on the device before the first timed call
+            ArrayHandle<double2> d0(r->p0, access_location::device, access_mode::read);
+            ArrayHandle<double2> d1(r->p1, access_location::device, access_mode::read);
+        }
+        if (cudaEventCreate(&r->e0) != cudaSuccess || cudaEventCreate(&r->e1) != cudaSuccess) return nullptr;
+        if (cudaDeviceSynchronize() != cudaSuccess) return nullptr;
+        return r;
+    } catch (...) {
+        return nullptr;
+    }
+}
+
+static int gpu_timed(RefGpu *r, bool build, float *ms)
+{
+    cudaEventRecord(r->e0, 0);
+    if (build) r->del->globalDelaunayTriangulation(r->p0, r->tri, r->nn);
+    else r->del->testAndRepairDelaunayTriangulation(r->p1, r->tri, r->nn);
+    cudaEventRecord(r->e1, 0);
+    if (cudaEventSynchronize(r->e1) != cudaSuccess) return -1;
+    if (cudaGetLastError() != cudaSuccess) return -1;
+    if (ms) cudaEventElapsedTime(ms, r->e0, r->e1);
+    return 0;
+}
+
+/* globalDelaunayTriangulation(p0) on the GPU; *ms = device time.  0, or -1 on error. */
+int ref_gpu_build(void *h, float *ms)
+{
+    try {
+        return gpu_timed(static_cast<RefGpu *>(h), true, ms);
+    } catch (...) {
+        return -1;
+    }
+}
+
+/* 1 when the class's current triangulation has exactly 2N triangles by smallest-index
+   ownership, ring sizes summing to 6N and every entry a valid index: the input the
+   triangle-list kernel can take without writing past its 2N-entry array. */
+int ref_gpu_triangles_ok(void *h)
+{
+    try {
+        RefGpu *r = static_cast<RefGpu *>(h);
+        const int n = r->n;
+        const long long rowlen = (long long)(r->tri.getNumElements() / n);
+        ArrayHandle<int> ht(r->tri, access_location::host, access_mode::read);
+        ArrayHandle<int> hn(r->nn, access_location::host, access_mode::read);
+        long long tris = 0, deg = 0;
+        for (int i = 0; i < n; ++i) {
+            const int m = hn.data[i];
+            if (m < 3 || m > rowlen) return 0;
+            deg += m;
+            const int *row = ht.data + (size_t)i * rowlen;
+            for (int k = 0; k < m; ++k)
+                if (row[k] < 0 || row[k] >= n) return 0;
+            int y = row[m - 1];
+            for (int k = 0; k < m; ++k) {
+                const int z = row[k];
+                if (i < y && i < z) tris++;
+                y = z;
+            }
+        }
+        return (tris == 2LL * n && deg == 6LL * n) ? 1 : 0;
+    } catch (...) {
+        return 0;
+    }
+}
+
+/* testAndRepairDelaunayTriangulation(p1) on the GPU, on the class's current triangulation;
+   refused (-2) unless ref_gpu_triangles_ok holds for it.  *ms = device time. */
+int ref_gpu_repair(void *h, float *ms)
+{
+    try {
+        if (ref_gpu_triangles_ok(h) != 1) return -2;
+        return gpu_timed(static_cast<RefGpu *>(h), false, ms);
+    } catch (...) {
+        return -1;
+    }
+}
+
+/* the class's current rings into tri (n x stride) and nn; returns its row length MaxSize */
+int ref_gpu_fetch(void *h, int *tri, int *nn, int stride)
+{
+    try {
+        RefGpu *r = static_cast<RefGpu *>(h);
+        const int rowlen = (int)(r->tri.getNumElements() / r->n);
+        ArrayHandle<int> ht(r->tri, access_location::host, access_mode::read);
+        ArrayHandle<int> hn(r->nn, access_location::host, access_mode::read);
+        for (int i = 0; i < r->n; ++i) {
+            nn[i] = hn.data[i];
+            for (int k = 0; k < std::min(rowlen, stride); ++k)
+                tri[(size_t)i * stride + k] = ht.data[(size_t)i * rowlen + k];
+        }
+        return rowlen;
+    } catch (...) {
+        return -1;
+    }
+}
+
+void ref_gpu_destroy(void *h)
+{
+    RefGpu *r = static_cast<RefGpu *>(h);
+    if (!r) return;
+    if (r->e0) cudaEventDestroy(r->e0);
+    if (r->e1) cudaEventDestroy(r->e1);
+    delete r->del;
+    delete r;
+}
 
 }  // extern "C"

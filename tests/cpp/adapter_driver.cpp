@@ -63,7 +63,7 @@ int main(int argc, char **argv)
         delGPU.testAndRepairDelaunayTriangulation(pts, tri, nn);
         dump(out, tri, nn, n);
         fclose(out);
-        printf("ok MaxSize=%d\n", delGPU.MaxSize());
+        printf("ok MaxSize=%d\n", delGPU.MaxSize);
     } catch (const std::exception &e) {
         fprintf(stderr, "error: %s\n", e.what());
         return 1;

@@ -70,7 +70,9 @@ def test_cpp_adapter_header_compiles(tmp_path):
                    'struct Box { void getBoxDims(double &a, double &b, double &c, double &d) const '
                    '{ a = 10; b = 5; c = 0; d = 8; } };\n'
                    'void use() { auto bx = std::make_shared<Box>(); dgt::DelaunayGPU g(100, 16, 1.0, bx); '
-                   'g.setBox(bx); }\nint main(){ return 0; }\n')
+                   'g.setBox(bx); int m = g.MaxSize; (void)m; dgt::DelaunayGPU b; b.initialize(100, 16, 1.0, bx); '
+                   'dgt::DelaunayGPUT<std::shared_ptr<Box>> k(100, 16, 1.0, bx); double a, c, d, e; '
+                   'k.Box->getBoxDims(a, c, d, e); }\nint main(){ return 0; }\n')
     cuda_inc = "/usr/local/cuda/include"
     r = subprocess.run(["g++", "-std=c++14", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), "-I", cuda_inc,
                         str(src)], capture_output=True, text=True)
@@ -86,3 +88,54 @@ def test_python_mirror_fails_loudly_without_device():
     with pytest.raises(N.DgtError) as e:
         DelaunayGPU(10, 16, 1.0, (3.0, 3.0))
     assert e.value.code == N.DGT_ERR_CUDA
+
+
+REFERENCE_USE = r"""
+#include "std_include.h"
+#include "gpuarray.h"
+#include "periodicBoundaries.h"
+#include "dgt_gpuarray.hpp"
+// the reference's driver code (triangulation.cpp:224-246, :299, :361, :390) over the adapter
+void use()
+{
+    PeriodicBoxPtr domain = make_shared<periodicBoundaries>(10.0, 10.0);
+    GPUArray<double2> gpuPts(100u);
+    GPUArray<int> gpuTriangulation(1600u), cellNeighborNumber(100u);
+    dgt::DelaunayGPUT<PeriodicBoxPtr> delGPU(100, 16, 1.0, domain);
+    delGPU.setSafetyMode(true);
+    delGPU.setGPUcompute(true);
+    delGPU.globalDelaunayTriangulation(gpuPts, gpuTriangulation, cellNeighborNumber);
+    double2 pTarget;
+    pTarget.x = 11.0;
+    pTarget.y = -1.0;
+    delGPU.Box->putInBoxReal(pTarget);
+    delGPU.testAndRepairDelaunayTriangulation(gpuPts, gpuTriangulation, cellNeighborNumber);
+    int maxSize = delGPU.MaxSize;
+    (void)maxSize;
+    delGPU.prof.print();
+    dgt::DelaunayGPU blank;
+    blank.initialize(100, 16, 1.0, domain);
+    blank.updateList(gpuPts);
+}
+int main() { return 0; }
+"""
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="no host C++ compiler")
+def test_cpp_adapter_compiles_against_reference_gpuarray(tmp_path):
+    # the GPUArray<T> traits (include/dgt_gpuarray.hpp) instantiated with the reference's own
+    # container and box headers, as a maintainer of the reference would build them
+    from oracle import oracle as O
+
+    ref = O.reference_dir()
+    if not os.path.exists(os.path.join(ref, "inc", "gpuarray.h")):
+        pytest.skip("the reference's sources are not present")
+    src = tmp_path / "use_gpuarray.cpp"
+    src.write_text(REFERENCE_USE)
+    cuda_inc = "/usr/local/cuda/include"
+    r = subprocess.run(["g++", "-std=c++14", "-fsyntax-only", "-DENABLE_CUDA",
+                        "-I", os.path.join(ref, "inc"), "-I", os.path.join(ref, "src"),
+                        "-I", os.path.join(ref, "src", "utilities"), "-I", os.path.join(ROOT, "include"),
+                        "-I", cuda_inc, "-I", os.path.join(cuda_inc, "nvtx3"), str(src)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
