@@ -38,6 +38,7 @@ EXPORTED = [
 ]
 STEP_AUTO = 0xFFFFFFFFFFFFFFFF
 NOALLOC_MAX_POINTS = 65536
+KERNEL_SHAPES = 7   # dgt_set_kernel_shape: 0..6 (include/dgt.h)
 PHASES = ["bin", "build", "slow", "test", "repair"]
 
 
@@ -98,7 +99,7 @@ class TuneResult(ctypes.Structure):
         ("best_ms", ctypes.c_float),
         ("default_ms", ctypes.c_float),
         ("from_cache", ctypes.c_int),
-        ("reserved", ctypes.c_int),
+        ("work_budget", ctypes.c_int),
     ]
 
     def as_dict(self):

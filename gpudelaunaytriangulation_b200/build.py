@@ -16,8 +16,9 @@ CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIBDIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(LIBDIR, "libdgt.so")
-SOURCES = ["dgt_bin.cu", "dgt_ring.cu", "dgt_flip.cu", "dgt_validate.cu", "dgt_api.cu", "dgt_noalloc.cu"]
-HEADERS = ["dgt_internal.cuh", "dgt_predicates.cuh", "dgt_rowreg.cuh"]
+SOURCES = ["dgt_bin.cu", "dgt_ring.cu", "dgt_group.cu", "dgt_flip.cu", "dgt_validate.cu", "dgt_api.cu",
+           "dgt_noalloc.cu"]
+HEADERS = ["dgt_internal.cuh", "dgt_predicates.cuh", "dgt_rowreg.cuh", "dgt_builder.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]

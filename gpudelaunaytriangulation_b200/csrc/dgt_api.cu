@@ -1127,9 +1127,14 @@ int dgt_get_tuning(const dgt_context *c, double *cell_size, int *shape, int *rin
 
 namespace {
 
-// tuned (cell size relative to the mean spacing, kernel shape) per class of input
+// tuned (cell size relative to the mean spacing, kernel shape, work budget) per class of input
 typedef std::tuple<int, int, int, int> TuneKey;   // log2 points, log2 sets, contrast class, precision
-std::map<TuneKey, std::pair<double, int>> g_tune_cache;
+struct TuneVal {
+    double rel;
+    int shape;
+    int budget;
+};
+std::map<TuneKey, TuneVal> g_tune_cache;
 std::mutex g_tune_mutex;
 
 __global__ void k_max_count(const int *ccount, int cells, int *out)
@@ -1177,7 +1182,7 @@ int dgt_autotune(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, 
     cudaStream_t s = (cudaStream_t)stream;
     const int safety = c->safety, timing = c->timing;
     const double cell0 = c->cell_size;
-    const int shape0 = c->shape;
+    const int shape0 = c->shape, budget0 = c->work_budget;
     c->safety = 1;
     c->timing = false;
     // density contrast of the input on the mean-spacing grid: largest cell count
@@ -1199,12 +1204,14 @@ int dgt_autotune(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, 
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         auto it = g_tune_cache.find(key);
         if (it != g_tune_cache.end()) {
-            set_relative_cell(c, it->second.first);
-            c->shape = it->second.second;
+            set_relative_cell(c, it->second.rel);
+            c->shape = it->second.shape;
+            c->work_budget = it->second.budget;
             c->safety = safety;
             c->timing = timing;
             out->cell_size = c->cell_size;
             out->shape = c->shape;
+            out->work_budget = c->work_budget;
             out->from_cache = 1;
             return init_context(c);
         }
@@ -1257,6 +1264,24 @@ int dgt_autotune(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, 
             best_shape = shape;
         }
     }
+    // clustered inputs: how long a point may scan in the per-thread kernel before the warp
+    // kernel takes it over (uniform inputs stay far below any of these)
+    int best_budget = budget0;
+    if (contrast == 2) {
+        const int budgets[] = { 512, 2048 };
+        for (int b : budgets) {
+            if (rr != DGT_OK) break;
+            float ms = 0;
+            c->work_budget = b;
+            rr = trial(best_rel, best_shape, &ms);
+            if (rr != DGT_OK) break;
+            if (ms < best) {
+                best = ms;
+                best_budget = b;
+            }
+        }
+        c->work_budget = best_budget;
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     c->safety = safety;
@@ -1264,17 +1289,20 @@ int dgt_autotune(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, 
     if (rr != DGT_OK) {
         c->cell_size = cell0;
         c->shape = shape0;
+        c->work_budget = budget0;
         init_context(c);
         return rr;
     }
     set_relative_cell(c, best_rel);
     c->shape = best_shape;
+    c->work_budget = best_budget;
     {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
-        g_tune_cache[key] = std::make_pair(best_rel, best_shape);
+        g_tune_cache[key] = TuneVal{ best_rel, best_shape, best_budget };
     }
     out->cell_size = c->cell_size;
     out->shape = best_shape;
+    out->work_budget = best_budget;
     out->best_ms = best;
     r = init_context(c);
     if (r != DGT_OK) return r;

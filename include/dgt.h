@@ -224,13 +224,14 @@ void dgt_md_graph_destroy(dgt_graph *graph);
 int dgt_clear_flags(dgt_context *ctx, void *stream);
 
 /* Kernel shape of the one-ring kernel: (ring entries kept on chip, threads per block) =
- * 0: (14, 64) default, 1: (12, 64), 2: (16, 64), 3: (14, 32), 4: (12, 32).  Rings longer than
- * the on-chip capacity continue on the deferred (warp-per-point) path, so every shape gives the same
- * output. */
+ * 0: (14, 64) default, 1: (12, 64), 2: (16, 64), 3: (14, 32), 4: (12, 32), one thread per
+ * point; 5: (14, 64) with a group of 4 lanes per point, 6: (14, 64) with 8 lanes per point.
+ * Rings longer than the on-chip capacity continue on the deferred (warp-per-point) path, so
+ * every shape gives the same output. */
 int dgt_set_kernel_shape(dgt_context *ctx, int shape);
 /* Work budget (no reference counterpart): cells plus candidates one point may scan in the
  * thread-per-point kernel before it is handed to the warp-per-point kernel (points on the rim
- * of dense clusters, whose circles reach over large regions).  Default 4096; 0 sends every
+ * of dense clusters, whose circles reach over large regions).  Default 1024; 0 sends every
  * point to the warp-per-point kernel.  Both kernels give the same rings. */
 int dgt_set_work_budget(dgt_context *ctx, int budget);
 /* Repair strategy (no reference counterpart): on (default), test-and-repair first flips the
@@ -257,7 +258,7 @@ typedef struct dgt_tune_result {
     float best_ms;      /* build time with the chosen settings */
     float default_ms;   /* build time with cell edge = mean spacing, shape 0 */
     int from_cache;
-    int reserved;
+    int work_budget;    /* chosen work budget of the per-thread kernel (dgt_set_work_budget) */
 } dgt_tune_result;
 int dgt_autotune(dgt_context *ctx, const double *d_points, int *d_tri, int *d_neighnum, int stride, void *stream,
                  dgt_tune_result *out);

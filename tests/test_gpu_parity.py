@@ -11,6 +11,7 @@ import os
 import numpy as np
 import pytest
 
+from gpudelaunaytriangulation_b200 import _native as N
 from gpudelaunaytriangulation_b200 import workloads as W
 from oracle import oracle as O
 
@@ -415,7 +416,7 @@ def test_every_kernel_shape_same_output():
     L = float(np.sqrt(n))
     pts = W.uniform_points(n, L, 111)
     ref = O.restated_global(pts, L, L, 1.0, 32)
-    for shape in range(5):
+    for shape in range(N.KERNEL_SHAPES):
         d = _dg()(n, 16, 1.0, (L, L))
         d.setKernelShape(shape)
         P = torch.from_numpy(pts).cuda()
@@ -434,7 +435,7 @@ def test_autotune_result_is_correct_and_cached():
     tri = torch.zeros(16 * n, dtype=torch.int32, device="cuda")
     nn = torch.zeros(n, dtype=torch.int32, device="cuda")
     res = d.autotune(P, tri, nn)
-    assert res["trials"] >= 5 and 0 <= res["shape"] < 5 and res["best_ms"] <= res["default_ms"] * 1.05
+    assert res["trials"] >= 5 and 0 <= res["shape"] < N.KERNEL_SHAPES and res["best_ms"] <= res["default_ms"] * 1.05
     t, k = host(tri, nn)
     assert_delaunay(pts, L, L, t, k, scan=False)
     d2 = _dg()(n, 16, 1.0, (L, L))
