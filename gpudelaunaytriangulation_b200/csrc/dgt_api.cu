@@ -434,10 +434,15 @@ cudaError_t run_deferred(dgt_context *c, const RingArgs &a, cudaStream_t s)
     return launch_deferred(a, c->sms, s);
 }
 
+// The kernel shape (and the autotuner's choice of it) applies to global triangulations; the
+// rebuild rounds of a repair take the default shape, which is the fastest for their short,
+// latency-bound work lists (measured: 256-set ensemble MD step 0.99 ms against 1.05 ms with
+// the shape tuned for its build; 4M-point repair 1.07 ms against 1.14 ms with shape 1)
 cudaError_t run_build(dgt_context *c, const RingArgs &a, cudaStream_t s)
 {
     c->launches += a.n_items > 0 ? 1 : 0;
-    return launch_build(a, c->precision == DGT_PRECISION_FP64 ? MODE_F64 : MODE_F32, c->sms, c->shape, s);
+    return launch_build(a, c->precision == DGT_PRECISION_FP64 ? MODE_F64 : MODE_F32, c->sms,
+                        a.repair ? 0 : c->shape, s);
 }
 
 void to_stats(const DevStatus &d, dgt_stats *o)
@@ -661,12 +666,27 @@ namespace {
 // batches and the host stops once a list is empty (needs a synchronisation per batch);
 // fixed_rounds > 0: exactly that many rounds, no host synchronisation (graph capture),
 // an unfinished queue sets DGT_FLAG_NOT_CONVERGED in the device flags.
+// An MD step's displacement, fused into the repair: one kernel moves and wraps every point
+// and measures how far it now lies outside the cell that lists it (the local test then skips
+// that measurement); the step counter advances at the end of the call.
+struct MdMove {
+    double sigma;
+    unsigned long long seed;
+};
+
 int repair_impl(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, int stride, cudaStream_t s,
-                int fixed_rounds, bool conclude_now)
+                int fixed_rounds, bool conclude_now, const MdMove *md = nullptr)
 {
     DevStatus *dst = c->st.as<DevStatus>();
     DevCtl *ctl = c->ctl.as<DevCtl>();
     DGT_TRY(cudaMemsetAsync(c->st.p, 0, sizeof(DevStatus), s));
+    const bool measured = md && c->flip && c->binned;
+    if (md) {
+        c->launches += 1;
+        DGT_TRY(launch_displace_md(reinterpret_cast<double2 *>(const_cast<double *>(d_points)), c->n,
+                                   c->d_sets.as<SetDesc>(), c->batch ? c->d_set_of.as<int>() : nullptr, md->sigma,
+                                   md->seed, &ctl->step, measured ? c->cell_of.as<int>() : nullptr, dst, s));
+    }
     // With the cell lists of an earlier binning of this grid, flip mode measures how far the
     // points left their cells in the local test and decides on rebinning only once the rebuild rounds
     // need the lists (they read candidate positions through the index, so the cell-order copy
@@ -693,7 +713,7 @@ int repair_impl(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, i
     t.flip_list = c->flip ? flips[0] : nullptr;
     t.flip_count = &dst->flip_count[0];
     t.flip_cap = c->flip_cap;
-    t.rcell_of = fold ? c->cell_of.as<int>() : nullptr;
+    t.rcell_of = (fold && !measured) ? c->cell_of.as<int>() : nullptr;
     t.general = c->general;
     t.st = dst;
     {
@@ -798,7 +818,7 @@ int repair_impl(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, i
     }
     phase_end(c, DGT_PHASE_REPAIR, s);
     c->launches += 1;
-    DGT_TRY(launch_call_end(ctl, dst, round, s));
+    DGT_TRY(launch_call_end(ctl, dst, round, s, md != nullptr));
     if (!conclude_now) return DGT_OK;
     return conclude(c, s, pending);
 }
@@ -978,12 +998,11 @@ int dgt_md_step(dgt_context *c, double *d_points, int *d_tri, int *d_nn, int str
     if (!c || rounds < 1 || rounds > 64) return DGT_ERR_INVALID_ARGUMENT;
     if (c->n == 0) return DGT_OK;
     if (!d_points || !d_tri || !d_nn || !valid_stride(stride)) return DGT_ERR_INVALID_ARGUMENT;
+    if (!(sigma >= 0) || !std::isfinite(sigma)) return DGT_ERR_INVALID_ARGUMENT;
     cudaStream_t s = (cudaStream_t)stream;
-    int r = dgt_displace(c, d_points, sigma, seed, DGT_STEP_AUTO, stream);
-    if (r != DGT_OK) return r;
     begin_call(c, s);
-    c->launches += 2;
-    return repair_impl(c, d_points, d_tri, d_nn, stride, s, rounds, false);
+    const MdMove md{ sigma, seed };
+    return repair_impl(c, d_points, d_tri, d_nn, stride, s, rounds, false, &md);
 }
 
 struct dgt_graph {

@@ -48,6 +48,11 @@ __global__ void __launch_bounds__(256) k_clear_counts(int *ccount, int ncell, in
     }
 }
 
+// The cell of every point and its rank among the points of that cell, plus the occupancy of
+// the 8 x 8-cell blocks.  (Warp-aggregated atomics, one per group of lanes sharing a cell via
+// __match_any_sync, were measured and left out: points arrive in index order, which is
+// spatially random even for the clustered inputs, so a warp almost never holds two points of
+// one cell, and the match made the 4M-point binning 0.26 -> 0.33 ms.)
 __global__ void __launch_bounds__(256) k_count(BinArgs a, DevStatus *st)
 {
     if (skip(a.cond)) return;
@@ -304,38 +309,51 @@ __device__ __forceinline__ double wrap_coord(double x, double L)
     return x;
 }
 
+// cell_of (MD steps of a context that holds a binning): the cell that lists each point; the
+// kernel then also measures how far the moved point lies outside that cell (the margin the
+// repair's certification needs while it keeps the cell lists, outside_cell) into
+// st->skin_measured, so the repair's local test does not have to
 __global__ void __launch_bounds__(256) k_displace(double2 *pos, int n, const SetDesc *sets, const int *set_of,
                                                   double sigma, unsigned long long seed, unsigned long long step,
-                                                  const unsigned long long *step_ptr)
+                                                  const unsigned long long *step_ptr, const int *cell_of,
+                                                  DevStatus *st)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    if (step_ptr) step = *step_ptr;
-    const SetDesc &S = sets[set_of ? set_of[i] : 0];
-    unsigned long long h = smix(seed ^ smix(step * 0x100000001B3ULL + (unsigned long long)i));
-    unsigned long long h2 = smix(h);
-    double u1 = ((h >> 11) + 1) * (1.0 / 9007199254740993.0);   // (0, 1]
-    double u2 = (h2 >> 11) * (1.0 / 9007199254740992.0);
-    double r = sigma * sqrt(-2.0 * log(u1));
-    double sn, cs;
-    sincospi(2.0 * u2, &sn, &cs);
-    double2 p = pos[i];
-    if (S.general) {
-        // periodicBoundaries::move (periodicBoundaries.h:181-189): displace, then back into
-        // the unit cell through fractional coordinates
-        p.x += r * cs;
-        p.y += r * sn;
-        double u = S.i11 * p.x + S.i12 * p.y, v = S.i21 * p.x + S.i22 * p.y;
-        u -= floor(u);
-        v -= floor(v);
-        if (!(u < 1.0)) u = 0.0;
-        if (!(v < 1.0)) v = 0.0;
-        p = make_double2(S.m11 * u + S.m12 * v, S.m21 * u + S.m22 * v);
-    } else {
-        p.x = wrap_coord(p.x + r * cs, S.Lx);
-        p.y = wrap_coord(p.y + r * sn, S.Ly);
+    float mv = 0.0f;
+    if (i < n) {
+        if (step_ptr) step = *step_ptr;
+        const SetDesc &S = sets[set_of ? set_of[i] : 0];
+        unsigned long long h = smix(seed ^ smix(step * 0x100000001B3ULL + (unsigned long long)i));
+        unsigned long long h2 = smix(h);
+        double u1 = ((h >> 11) + 1) * (1.0 / 9007199254740993.0);   // (0, 1]
+        double u2 = (h2 >> 11) * (1.0 / 9007199254740992.0);
+        double r = sigma * sqrt(-2.0 * log(u1));
+        double sn, cs;
+        sincospi(2.0 * u2, &sn, &cs);
+        double2 p = pos[i];
+        if (S.general) {
+            // periodicBoundaries::move (periodicBoundaries.h:181-189): displace, then back into
+            // the unit cell through fractional coordinates
+            p.x += r * cs;
+            p.y += r * sn;
+            double u = S.i11 * p.x + S.i12 * p.y, v = S.i21 * p.x + S.i22 * p.y;
+            u -= floor(u);
+            v -= floor(v);
+            if (!(u < 1.0)) u = 0.0;
+            if (!(v < 1.0)) v = 0.0;
+            p = make_double2(S.m11 * u + S.m12 * v, S.m21 * u + S.m22 * v);
+        } else {
+            p.x = wrap_coord(p.x + r * cs, S.Lx);
+            p.y = wrap_coord(p.y + r * sn, S.Ly);
     }
     pos[i] = p;
+    if (cell_of) mv = S.general ? outside_cell<true>(S, cell_of[i], p) : outside_cell<false>(S, cell_of[i], p);
+    }
+    if (cell_of) {
+        for (int o = 16; o > 0; o >>= 1) mv = fmaxf(mv, __shfl_down_sync(0xffffffffu, mv, o));
+        if ((threadIdx.x & 31) == 0 && mv > 0.0f)
+            atomicMax(reinterpret_cast<int *>(&st->skin_measured), __float_as_int(mv));
+    }
 }
 
 __global__ void k_advance_step(unsigned long long *step_ptr) { *step_ptr += 1; }
@@ -345,8 +363,17 @@ cudaError_t launch_displace(double2 *pos, int n, const SetDesc *sets, const int 
                             cudaStream_t s)
 {
     if (n <= 0) return cudaSuccess;
-    k_displace<<<(n + 255) / 256, 256, 0, s>>>(pos, n, sets, set_of, sigma, seed, step, step_ptr);
+    k_displace<<<(n + 255) / 256, 256, 0, s>>>(pos, n, sets, set_of, sigma, seed, step, step_ptr, nullptr, nullptr);
     if (step_ptr) k_advance_step<<<1, 1, 0, s>>>(step_ptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_displace_md(double2 *pos, int n, const SetDesc *sets, const int *set_of, double sigma,
+                               unsigned long long seed, unsigned long long *step_ptr, const int *cell_of,
+                               DevStatus *st, cudaStream_t s)
+{
+    if (n <= 0) return cudaSuccess;
+    k_displace<<<(n + 255) / 256, 256, 0, s>>>(pos, n, sets, set_of, sigma, seed, 0ull, step_ptr, cell_of, st);
     return cudaGetLastError();
 }
 

@@ -316,9 +316,15 @@ cudaError_t launch_restride(const int *src, int old_stride, int *dst, int new_st
 cudaError_t launch_displace(double2 *pos, int n, const SetDesc *sets, const int *set_of, double sigma,
                             unsigned long long seed, unsigned long long step, unsigned long long *step_ptr,
                             cudaStream_t s);
+// MD step: displacement + wrap, and (cell_of != null) the distance each moved point lies
+// outside the cell that lists it, into st->skin_measured (st cleared beforehand); the step is
+// read from *step_ptr and advanced by the end of the call (launch_call_end, advance_step)
+cudaError_t launch_displace_md(double2 *pos, int n, const SetDesc *sets, const int *set_of, double sigma,
+                               unsigned long long seed, unsigned long long *step_ptr, const int *cell_of,
+                               DevStatus *st, cudaStream_t s);
 // end of a test-and-repair call: fold flags into the sticky word, check convergence,
-// advance the epoch by rounds + 1
-cudaError_t launch_call_end(DevCtl *ctl, DevStatus *st, int rounds, cudaStream_t s);
+// advance the epoch by rounds + 1 (and the displacement step counter when advance_step)
+cudaError_t launch_call_end(DevCtl *ctl, DevStatus *st, int rounds, cudaStream_t s, bool advance_step = false);
 // first rebuild round of a flip-mode repair: the current ring neighbours of its points join it
 cudaError_t launch_expand(int *list, int *count, int cap, const int *tri, const int *nn, int stride, int n,
                           int *mark, const int *epoch_ptr, int sms, cudaStream_t s);

@@ -623,8 +623,9 @@ cudaError_t launch_expand(int *list, int *count, int cap, const int *tri, const 
     return cudaGetLastError();
 }
 
-__global__ void k_call_end(DevCtl *ctl, DevStatus *st, int rounds)
+__global__ void k_call_end(DevCtl *ctl, DevStatus *st, int rounds, int advance_step)
 {
+    if (advance_step) ctl->step += 1;
     int f = st->err_flags;
     if (rounds > 0) {
         if (st->list_count[rounds & 1] > 0) {
@@ -637,9 +638,9 @@ __global__ void k_call_end(DevCtl *ctl, DevStatus *st, int rounds)
     ctl->sticky |= f;
 }
 
-cudaError_t launch_call_end(DevCtl *ctl, DevStatus *st, int rounds, cudaStream_t s)
+cudaError_t launch_call_end(DevCtl *ctl, DevStatus *st, int rounds, cudaStream_t s, bool advance_step)
 {
-    k_call_end<<<1, 1, 0, s>>>(ctl, st, rounds);
+    k_call_end<<<1, 1, 0, s>>>(ctl, st, rounds, advance_step ? 1 : 0);
     return cudaGetLastError();
 }
 

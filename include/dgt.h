@@ -227,7 +227,8 @@ int dgt_clear_flags(dgt_context *ctx, void *stream);
  * 0: (14, 64) default, 1: (12, 64), 2: (16, 64), 3: (14, 32), 4: (12, 32), one thread per
  * point; 5: (14, 64) with a group of 4 lanes per point, 6: (14, 64) with 8 lanes per point.
  * Rings longer than the on-chip capacity continue on the deferred (warp-per-point) path, so
- * every shape gives the same output. */
+ * every shape gives the same output.  The shape applies to global triangulations; the
+ * rebuild rounds of test-and-repair always take shape 0. */
 int dgt_set_kernel_shape(dgt_context *ctx, int shape);
 /* Work budget (no reference counterpart): cells plus candidates one point may scan in the
  * thread-per-point kernel before it is handed to the warp-per-point kernel (points on the rim
