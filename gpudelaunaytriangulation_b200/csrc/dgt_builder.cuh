@@ -344,6 +344,61 @@ struct Builder {
         return R_OK;
     }
 
+    // One ring edge k against candidate d (float offset) / d64 (double offset): 1 strictly
+    // inside its circle, 0 not, -1 undecided even in float64 (only without EXACT).  The
+    // filter of classify for a single edge, with the same recheck and check-mode accounting.
+    __device__ __forceinline__ int test_edge(int k, V2 d, double2 d64)
+    {
+        const T nd = d.x * d.x + d.y * d.y;
+        const T ad = sqrt_up(nd);
+        const T kb = (T)8 * PR::u() * nd + PR::tiny();
+        const E4 e = R.edge(k);
+        const T sv = fma(d.x, e.x, fma(d.y, e.y, -nd));
+        const T bd = fma(ad, e.z, kb);
+        ctr.tests++;
+        if (sv > bd || sv < -bd) {
+            const int in = sv > bd ? 1 : 0;
+            if (A.check) {
+                const int ia = R.idx(k), ib = R.idx(k + 1 == m ? 0 : k + 1);
+                ctr.add_mism(GEN ? check64g(A.pos, p, Sg, ia, ib, d64.x, d64.y, in)
+                                 : check64(A.pos, p, S.Lx, S.hLx, S.Ly, S.hLy, S.V, ia, ib, d64.x, d64.y, in));
+            }
+            return in;
+        }
+        ctr.add_u32();
+        const int r = recheck(k, d64);
+        return r == 0 ? -1 : (r > 0 ? 1 : 0);
+    }
+
+    // The conflict arc of `mask` on a ring of m entries: first edge s, last edge e (s > e when
+    // it wraps past the end), count c; false when the conflicting edges are not one arc.
+    __device__ __forceinline__ static bool conflict_arc(Mask mask, int m, int &s, int &e, int &c)
+    {
+        const Mask full = (m == 8 * (int)sizeof(Mask)) ? ~(Mask)0 : (((Mask)1 << m) - 1);
+        const Mask nm = ~mask & full;
+        const Mask rl = ((nm << 1) | (nm >> (m - 1))) & full;
+        const Mask rr = ((nm >> 1) | (nm << (m - 1))) & full;
+        const Mask starts = mask & rl, ends = mask & rr;
+        s = ffs_(starts) - 1;
+        e = ffs_(ends) - 1;
+        c = popc_(mask);
+        return mask != full && popc_(starts) == 1;
+    }
+    // After inserting a candidate over arc [s, e]: another candidate's decisions for the
+    // edges that survive (same circles) at their new indices; the two new edges start at
+    // the returned index (their bits are left clear).
+    __device__ __forceinline__ static Mask remap_mask(Mask mk, int s, int e, int &ns)
+    {
+        if (s <= e) {
+            ns = s;
+            const Mask low = s == 0 ? (Mask)0 : ((((Mask)1 << s) - 1) & mk);
+            return low | ((mk >> (e + 1)) << (s + 2));
+        }
+        ns = s - e - 1;
+        const Mask keep = ns == 0 ? (Mask)0 : (((Mask)1 << ns) - 1);
+        return (mk >> (e + 1)) & keep;
+    }
+
     // one candidate: classify, insert on conflict
     __device__ __forceinline__ int candidate(int sl)
     {

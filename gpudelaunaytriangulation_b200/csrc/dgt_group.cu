@@ -47,46 +47,11 @@ template <int G> __device__ __forceinline__ unsigned gvote(bool p)
     return (b >> base) & ((1u << G) - 1u);
 }
 
-template <typename M> __device__ __forceinline__ M lowmask(int n)
-{
-    return n >= (int)(8 * sizeof(M)) ? ~(M)0 : (((M)1 << n) - 1);
-}
-
 // nearest-first key: the candidate's squared distance (non-negative float: its bit pattern
 // orders like the value) with the lane in the low bits
 template <int G> __device__ __forceinline__ unsigned near_key(float nd, int glane)
 {
     return (__float_as_uint(nd) & ~(unsigned)(G - 1)) | (unsigned)glane;
-}
-
-// One ring edge k against a candidate: 1 strictly inside its circle, 0 not, -1 undecided
-// even in float64 (the point goes to the exact path).  Float32 filter, then float64 recheck;
-// in check mode a decided filter result is re-evaluated in float64 and contradictions counted.
-template <class B>
-__device__ __forceinline__ int edge_inside(B &b, int k, typename B::V2 d, double2 d64)
-{
-    typedef typename B::Real T;
-    typedef typename B::PR PR;
-    const T nd = d.x * d.x + d.y * d.y;
-    const T ad = sqrt_up(nd);
-    const T kb = (T)8 * PR::u() * nd + PR::tiny();
-    const typename B::E4 e = b.R.edge(k);
-    const T sv = fma(d.x, e.x, fma(d.y, e.y, -nd));
-    const T bd = fma(ad, e.z, kb);
-    b.ctr.tests++;
-    if (sv > bd || sv < -bd) {
-        const int in = sv > bd ? 1 : 0;
-        if (b.A.check) {
-            const int ia = b.R.idx(k), ib = b.R.idx(k + 1 == b.m ? 0 : k + 1);
-            b.ctr.add_mism(B::general ? check64g(b.A.pos, b.p, b.Sg, ia, ib, d64.x, d64.y, in)
-                                      : check64(b.A.pos, b.p, b.S.Lx, b.S.hLx, b.S.Ly, b.S.hLy, b.S.V, ia, ib,
-                                                d64.x, d64.y, in));
-        }
-        return in;
-    }
-    b.ctr.add_u32();
-    const int r = b.recheck(k, d64);
-    return r == 0 ? -1 : (r > 0 ? 1 : 0);
 }
 
 // The group inserts candidate (d, id) whose conflicting edges are `mask` (the same on every
@@ -97,22 +62,15 @@ template <int G, class B>
 __device__ __forceinline__ int grp_insert(B &b, bool go, int glane, typename B::V2 d, int id,
                                           typename B::Mask mask, int &s, int &e, int &ns)
 {
-    typedef typename B::Mask Mask;
     typedef typename B::V2 V2;
     typedef typename B::E4 E4;
     typedef typename B::Real T;
     constexpr int CAP = B::RingT::cap;
     const int m = b.m;
-    const Mask full = lowmask<Mask>(m);
-    const Mask nm = ~mask & full;
-    const Mask rl = ((nm << 1) | (nm >> (m - 1))) & full;
-    const Mask rr = ((nm >> 1) | (nm << (m - 1))) & full;
-    const Mask starts = mask & rl, ends = mask & rr;
+    int c;
+    const bool arc = B::conflict_arc(mask, m, s, e, c);
     int r = R_OK;
-    if (go && (mask == full || popc_(starts) != 1)) r = R_NONCONTIG;
-    s = ffs_(starts) - 1;
-    e = ffs_(ends) - 1;
-    const int c = popc_(mask);
+    if (go && !arc) r = R_NONCONTIG;
     const int mnew = m - c + 2;
     if (go && r == R_OK && mnew > CAP) r = R_CAPACITY;
     go = go && r == R_OK;
@@ -324,10 +282,10 @@ __device__ int grp_build(B &b, const bool act, const int glane)
                     int rr = R_OK;
                     if (want) {
                         // edges outside the inserted arc keep their circles (and decisions)
-                        Mask nmk = s <= e ? (Mask)((mask & lowmask<Mask>(s)) | ((mask >> (e + 1)) << (s + 2)))
-                                          : (Mask)((mask >> (e + 1)) & lowmask<Mask>(s - e - 1));
-                        const int i0 = edge_inside(b, ns, d, d64);
-                        const int i1 = edge_inside(b, ns + 1, d, d64);
+                        int ns2;
+                        Mask nmk = B::remap_mask(mask, s, e, ns2);
+                        const int i0 = b.test_edge(ns, d, d64);
+                        const int i1 = b.test_edge(ns + 1, d, d64);
                         if (i0 < 0 || i1 < 0) rr = R_EXACT;
                         nmk |= (Mask)(i0 > 0) << ns;
                         nmk |= (Mask)(i1 > 0) << (ns + 1);

@@ -135,13 +135,23 @@ __device__ int coop_run(B &b, const int lane)
 
     // one candidate per lane (have): classify all, then insert the conflicting ones one at a
     // time (the others re-test against each new ring)
+    // one candidate per lane (have): classify all, then insert the conflicting ones one at a
+    // time, nearest first (a near candidate is the likelier Delaunay neighbour, and inserting
+    // it shrinks the circles the farther ones conflict with); after each insertion the others
+    // keep their decisions for the surviving edges and test only the two new ones
     auto settle = [&](int sl, bool have) {
         V2 d = B::PR::mk2(0, 0);
+        double2 d64 = make_double2(0.0, 0.0);
         Mask mask = 0;
-        if (have) b.classify(sl, d, mask);
+        if (have) b.classify(sl, d, mask, d64);
         unsigned want = __ballot_sync(0xffffffffu, have && mask != 0);
         while (want) {
-            const int leader = __ffs(want) - 1;
+            const float nd = (float)(d.x * d.x + d.y * d.y);
+            unsigned key = ((want >> lane) & 1u) ? ((__float_as_uint(nd) & ~31u) | (unsigned)lane) : 0xffffffffu;
+            for (int o = 16; o > 0; o >>= 1) key = min(key, __shfl_xor_sync(0xffffffffu, key, o));
+            const int leader = (int)(key & 31u);
+            const int m_old = b.m;
+            const Mask lmask = __shfl_sync(0xffffffffu, mask, leader);
             int ir = R_OK;
             if (lane == leader) ir = b.insert(d, __ldg(&A.sidx[sl]), mask);
             ir = __shfl_sync(0xffffffffu, ir, leader);
@@ -154,8 +164,16 @@ __device__ int coop_run(B &b, const int lane)
             }
             changed = true;
             const bool again = ((want >> lane) & 1u) && lane != leader;
-            mask = 0;
-            if (again) b.classify(sl, d, mask);
+            if (again) {
+                int s, e, c, ns;
+                B::conflict_arc(lmask, m_old, s, e, c);
+                mask = B::remap_mask(mask, s, e, ns);
+                const int i0 = b.test_edge(ns, d, d64), i1 = b.test_edge(ns + 1, d, d64);
+                mask |= (Mask)(i0 > 0) << ns;
+                mask |= (Mask)(i1 > 0) << (ns + 1);
+            } else {
+                mask = 0;
+            }
             want = __ballot_sync(0xffffffffu, again && mask != 0);
         }
     };
