@@ -52,7 +52,7 @@ BUILD_BYTES_PER_POINT = 16 + 4 + 4 + 24 + 4
 # dram__bytes_write.sum of one launch / points) on a 1,048,576-point capture of the same
 # kernel (the --profile build case below); traffic scales with the number of points at fixed
 # density, so the 4M launch is reported as this figure times its points.
-BUILD_DRAM_BYTES_PER_POINT_NCU = 87.2
+BUILD_DRAM_BYTES_PER_POINT_NCU = 87.5
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -682,13 +682,32 @@ def run_profile_case(args):
     triangulations of n seeded uniform points at unit density (build, repair), or in a
     general 60-degree box at unit density (hex); with `repair`, one test-and-repair after a
     sigma = 0.02 displacement.  Launch order per triangulation: 6 binning kernels, k_build,
-    k_build_warp.  Prints the counters of the calls."""
+    k_build_warp.  `md`: the 256-set ensemble, one build, then `--reps` MD steps.  Prints the
+    counters of the calls."""
     import math
 
     import torch
 
-    from gpudelaunaytriangulation_b200.delaunay import DelaunayGPU
+    from gpudelaunaytriangulation_b200.delaunay import DelaunayBatch, DelaunayGPU
 
+    if args.profile == "md":
+        # the batched ensemble of the ensemble_md measurement: 256 sets, one build, then
+        # `--reps` MD steps (sigma 0.01, 4 rebuild rounds) launched directly, not from a graph
+        pts, sizes, boxes = W.ensemble(256, 1000, 65536, seed=7)
+        n = len(pts)
+        b = DelaunayBatch(sizes, boxes, 16, 1.0)
+        P = torch.from_numpy(pts).cuda()
+        tri = torch.zeros(16 * n, dtype=torch.int32, device="cuda")
+        nn = torch.zeros(n, dtype=torch.int32, device="cuda")
+        b.globalDelaunayTriangulation(P, tri, nn)
+        stream = torch.cuda.Stream()
+        stream.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(stream):
+            for _ in range(args.reps):
+                b.mdStep(P, tri, nn, 0.01, seed=8, rounds=4, stream=stream)
+            stream.synchronize()
+        print(json.dumps({"md": b.stats()}))
+        return 0
     n = args.n or (1 << 20)
     L = math.sqrt(n)
     if args.profile == "hex":
@@ -730,7 +749,7 @@ def main():
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble MD measurement")
     ap.add_argument("--no-configs", action="store_true", help="skip the other workload families")
     ap.add_argument("--no-reference-gpu", action="store_true", help="skip timing the reference's own CUDA kernels")
-    ap.add_argument("--profile", choices=["build", "repair", "hex"], default=None,
+    ap.add_argument("--profile", choices=["build", "repair", "hex", "md"], default=None,
                     help="profiling case for Nsight Compute: a fixed, small sequence of calls (no timing)")
     ap.add_argument("--reps", type=int, default=2, help="global triangulations per --profile run")
     args = ap.parse_args()
