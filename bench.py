@@ -543,7 +543,7 @@ def run_ours(args):
         used = [None, None]   # compute finished with the step's positions
         out = [None, None]    # downloads of the step's results finished
         ready = [None, None]  # the step's positions uploaded
-        e_steps = max(20, args.steps)   # pipeline fill + drain (one upload, one download) amortised
+        e_steps = max(40, args.steps)   # pipeline fill + drain (one upload, one download) amortised
 
         def upload(k):
             # issued one step ahead, so it overlaps the previous step's calls

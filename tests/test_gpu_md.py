@@ -83,3 +83,25 @@ def test_unfinished_repair_is_flagged_not_hidden():
     b.mdStep(P, tri, nn, 0.3, seed=1, rounds=1)
     torch.cuda.synchronize()
     assert b.stats()["sticky_flags"] & 64
+
+
+def test_fused_md_step_equals_displacement_then_repair():
+    # dgt_md_step moves the points inside the repair call (one kernel: move, wrap, distance
+    # outside the listing cell); a separate dgt_displace followed by test-and-repair must
+    # give the same positions and the same rings, step after step
+    b1, P1, tri1, nn1, sizes, boxes = setup(num_sets=6, lo=1000, hi=6000, seed=24)
+    b2, P2, tri2, nn2, _, _ = setup(num_sets=6, lo=1000, hi=6000, seed=24)
+    for step in range(4):
+        b1.mdStep(P1, tri1, nn1, 0.02, seed=11, rounds=6)
+        b2.displace(P2, 0.02, seed=11, step=step)
+        b2.testAndRepairDelaunayTriangulation(P2, tri2, nn2)
+        torch.cuda.synchronize()
+        assert torch.equal(P1, P2), step
+        assert torch.equal(nn1, nn2), step
+    assert b1.stats()["sticky_flags"] == 0 and b1.stats()["md_step"] == 4
+    check_sets(P1, tri1, nn1, sizes, boxes)
+    n = nn1.numel()
+    t1 = tri1.view(n, -1).cpu().numpy()
+    t2 = tri2.view(n, -1).cpu().numpy()
+    k = nn1.cpu().numpy()
+    assert np.array_equal(O.canonical(t1, k), O.canonical(t2, k))
