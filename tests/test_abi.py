@@ -139,3 +139,41 @@ def test_cpp_adapter_compiles_against_reference_gpuarray(tmp_path):
                         "-I", cuda_inc, "-I", os.path.join(cuda_inc, "nvtx3"), str(src)],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="no host C++ compiler")
+def test_adapter_box_wraps_points_like_the_reference(tmp_path):
+    # dgt::BoxDims::putInBoxReal (the adapter's copy of the box, host code) puts points into
+    # the primary cell the way periodicBoundaries::putInBoxReal does, for rectangular and
+    # general boxes; no device involved
+    src = tmp_path / "box.cpp"
+    src.write_text(r"""
+#include <cstdio>
+#include "dgt_delaunay.hpp"
+int main()
+{
+    dgt::BoxDims r(10.0, 0.0, 0.0, 8.0), g(10.0, 5.0, 0.0, 8.0);
+    const double in[6][2] = { {-1.0, 3.0}, {10.0, 8.0}, {25.5, -17.25}, {3.0, 4.0}, {-1e-12, 7.999999999}, {1e6, -1e6} };
+    for (int k = 0; k < 6; ++k) {
+        double2 p; p.x = in[k][0]; p.y = in[k][1];
+        double2 q = p;
+        r.putInBoxReal(p);
+        g.putInBoxReal(q);
+        // fractional coordinates of q in the general box
+        const double det = 10.0 * 8.0 - 5.0 * 0.0;
+        const double u = (8.0 * q.x - 5.0 * q.y) / det, v = (-0.0 * q.x + 10.0 * q.y) / det;
+        std::printf("%.17g %.17g %.17g %.17g\n", p.x, p.y, u, v);
+    }
+    return 0;
+}
+""")
+    exe = tmp_path / "box"
+    r = subprocess.run(["g++", "-std=c++14", "-O1", "-I", os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include",
+                        str(src), "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    rows = [list(map(float, ln.split())) for ln in out if ln.strip()]
+    for x, y, u, v in rows:
+        assert 0.0 <= x < 10.0 and 0.0 <= y < 8.0
+        assert -1e-12 <= u < 1.0 + 1e-12 and -1e-12 <= v < 1.0 + 1e-12
+    assert rows[0][:2] == [9.0, 3.0] and rows[3][:2] == [3.0, 4.0]

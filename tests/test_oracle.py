@@ -149,3 +149,17 @@ def test_offsets_single_rounding():
 
     ex = [F(2047.8) - F(L) - F(0.3), F(0.3) - (F(2047.9) - F(L))]
     assert out[0] == float(ex[0]) and out[1] == float(ex[1])
+
+
+@pytest.mark.skipif(O.ref_lib() is None, reason="oracle/_ref not built (reference sources absent)")
+def test_reference_seed_pass_guard_measures_polygons():
+    # the guard bench.py runs before the reference's own CUDA kernels: the reference's seed
+    # pass, on the host, over the same points; its polygons must stay well inside the
+    # reference's rows (it has no capacity check there), and the measurement must flag a row
+    # width it reaches
+    n = 20000
+    L = float(np.sqrt(n))
+    pts = W.uniform_points(n, L, 2026)
+    mx = O.reference_seed_max(pts, L, L, 1.0, 64)
+    assert 4 <= mx <= 12
+    assert O.reference_seed_max(pts, L, L, 1.0, mx) == -1
