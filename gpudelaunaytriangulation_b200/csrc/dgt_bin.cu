@@ -49,10 +49,11 @@ __global__ void __launch_bounds__(256) k_clear_counts(int *ccount, int ncell, in
 }
 
 // The cell of every point and its rank among the points of that cell, plus the occupancy of
-// the 8 x 8-cell blocks.  (Warp-aggregated atomics, one per group of lanes sharing a cell via
-// __match_any_sync, were measured and left out: points arrive in index order, which is
-// spatially random even for the clustered inputs, so a warp almost never holds two points of
-// one cell, and the match made the 4M-point binning 0.26 -> 0.33 ms.)
+// the 8 x 8-cell blocks and of the 64 x 64-cell super-blocks.  (Warp-aggregated atomics, one
+// per group of lanes sharing a cell via __match_any_sync, were measured and left out: points
+// arrive in index order, which is spatially random even for the clustered inputs, so a warp
+// almost never holds two points of one cell, and the match made the 4M-point binning 0.26 ->
+// 0.33 ms.)
 __global__ void __launch_bounds__(256) k_count(BinArgs a, DevStatus *st)
 {
     if (skip(a.cond)) return;
@@ -67,7 +68,9 @@ __global__ void __launch_bounds__(256) k_count(BinArgs a, DevStatus *st)
         a.cell_of[i] = c;
         a.rank[i] = atomicAdd(&a.ccount[c], 1);
         int lc = c - S.cell_base, cy = lc / S.xsize, cx = lc - cy * S.xsize;
-        atomicAdd(&a.bcount[S.block_base + (cy >> BLOCK_SHIFT) * S.bxsize + (cx >> BLOCK_SHIFT)], 1);
+        // the first point of a block marks its super-block (one atomic per non-empty block)
+        if (atomicAdd(&a.bcount[S.block_base + (cy >> BLOCK_SHIFT) * S.bxsize + (cx >> BLOCK_SHIFT)], 1) == 0)
+            atomicAdd(&a.bcount[S.sblock_base + (cy >> SBLOCK_SHIFT) * S.sbxsize + (cx >> SBLOCK_SHIFT)], 1);
     }
 }
 

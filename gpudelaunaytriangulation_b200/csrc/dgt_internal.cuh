@@ -30,6 +30,9 @@ struct SetDesc {
     int bxsize;         // occupancy blocks per row (BLOCK_CELLS x BLOCK_CELLS cells each)
     int bysize;
     int block_base;     // first block of the set in the block-count array
+    int sbxsize;        // occupancy super-blocks per row (SBLOCK_CELLS x SBLOCK_CELLS cells each)
+    int sbysize;
+    int sblock_base;    // first super-block of the set in the block-count array
     // General periodic box (periodicBoundaries::setGeneral, periodicBoundaries.h:86-101): a
     // point is M u with u its fractional coordinates, and the cell grid is a grid over u, so
     // a cell is a parallelogram.  Used by the kernels' general-box instantiations only; the
@@ -45,14 +48,20 @@ struct SetDesc {
 
 constexpr int BLOCK_SHIFT = 3;   // occupancy blocks of 8 x 8 cells
 constexpr int BLOCK_CELLS = 1 << BLOCK_SHIFT;
+constexpr int SBLOCK_SHIFT = 6;  // occupancy super-blocks of 64 x 64 cells (8 x 8 blocks)
+constexpr int SBLOCK_CELLS = 1 << SBLOCK_SHIFT;
 
-// block grid of a set whose cell grid is already set; returns the number of blocks
+// block and super-block grids of a set whose cell grid is already set, at block_base of the
+// block-count array (the set's blocks, then its super-blocks); returns the number of entries
 inline int set_block_grid(SetDesc &S, int block_base)
 {
     S.bxsize = (S.xsize + BLOCK_CELLS - 1) / BLOCK_CELLS;
     S.bysize = (S.ysize + BLOCK_CELLS - 1) / BLOCK_CELLS;
     S.block_base = block_base;
-    return S.bxsize * S.bysize;
+    S.sbxsize = (S.xsize + SBLOCK_CELLS - 1) / SBLOCK_CELLS;
+    S.sbysize = (S.ysize + SBLOCK_CELLS - 1) / SBLOCK_CELLS;
+    S.sblock_base = block_base + S.bxsize * S.bysize;
+    return S.bxsize * S.bysize + S.sbxsize * S.sbysize;
 }
 
 // Distance on a periodic axis of `size` cells from u (cell units) to cell [c, c + 1].
@@ -175,7 +184,7 @@ struct BinArgs {
     int total_cells;
     int *ccount;     // total_cells + 1
     int *cstart;     // total_cells + 1
-    int *bcount;     // points per occupancy block (zeroed by the caller)
+    int *bcount;     // points per occupancy block, then non-empty blocks per super-block (zeroed by the caller)
     int *cell_of;    // n
     int *rank;       // n
     int *sidx, *slot_of;
@@ -193,7 +202,8 @@ struct RingArgs {
     const int *sidx;
     const int *slot_of;
     const int *cstart;
-    const int *bcount;  // points per occupancy block: empty blocks are skipped by the scan
+    const int *bcount;  // points per occupancy block, then non-empty blocks per super-block:
+                        // empty ones are skipped by the scan
     int *tri;
     int *nn;
     int stride;

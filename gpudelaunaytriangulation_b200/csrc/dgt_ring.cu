@@ -116,6 +116,57 @@ __device__ __forceinline__ void grow_axis(int a0, int a1, int lo, int hi, int st
     g1 = a1 + want_hi;
 }
 
+// j-th index of [0, len) in the order c, c + 1, c - 1, c + 2, c - 2, ... (the longer side
+// continues alone once the shorter one is used up)
+__device__ __forceinline__ int around(int j, int c, int len)
+{
+    const int lo = c, hi = len - 1 - c, m = min(lo, hi);
+    if (j <= 2 * m) return (j & 1) ? c + (j + 1) / 2 : c - j / 2;
+    const int off = j - m;
+    return hi > lo ? c + off : c - off;
+}
+
+// Tile ti of the strip [xa, xb] x [ya, yb] (cells relative to the own cell) cut into tiles of
+// 2^sh x 2^sh cells, nearest first: the strip's tile columns (left / right strip, q = 0 / 1)
+// or rows (bottom / top strip, q = 2 / 3) from the old rectangle outwards, and along each of
+// them from the tile level with the own cell outwards in both directions
+__device__ __forceinline__ void strip_tile(int ti, int q, int xa, int xb, int ya, int yb, int sh, int &ta, int &tb,
+                                           int &tc, int &td)
+{
+    const int tw = ((xb - xa) >> sh) + 1, th = ((yb - ya) >> sh) + 1;
+    int ix, iy;
+    if (q < 2) {
+        const int o = ti / th, c = min(max((0 - ya) >> sh, 0), th - 1);
+        ix = q == 0 ? tw - 1 - o : o;
+        iy = around(ti - o * th, c, th);
+    } else {
+        const int o = ti / tw, c = min(max((0 - xa) >> sh, 0), tw - 1);
+        iy = q == 2 ? th - 1 - o : o;
+        ix = around(ti - o * tw, c, tw);
+    }
+    ta = xa + (ix << sh);
+    tb = min(ta + (1 << sh) - 1, xb);
+    tc = ya + (iy << sh);
+    td = min(tc + (1 << sh) - 1, yb);
+}
+
+// Whether any occupancy entry of 2^sh x 2^sh cells (row-major from `base`, `row` per row)
+// that the cells [xa, xb] x [ya, yb] relative to (ocx, ocy), wrapped, touch holds points
+__device__ __forceinline__ bool occupied(const int *cnt, int base, int row, int sh, const SetDesc &S, int ocx, int ocy,
+                                         int xa, int xb, int ya, int yb)
+{
+    for (int xs = xa; xs <= xb;) {
+        const int ax = wrapi(ocx + xs, S.xsize), bx = ax >> sh;
+        for (int ys = ya; ys <= yb;) {
+            const int ay = wrapi(ocy + ys, S.ysize), by = ay >> sh;
+            if (__ldg(&cnt[base + by * row + bx]) != 0) return true;
+            ys += min((by + 1) << sh, S.ysize) - ay;
+        }
+        xs += min((bx + 1) << sh, S.xsize) - ax;
+    }
+    return false;
+}
+
 template <class B>
 __device__ int coop_run(B &b, const int lane)
 {
@@ -130,11 +181,9 @@ __device__ int coop_run(B &b, const int lane)
     const double fx = fp.x - (double)b.ocx, fy = fp.y - (double)b.ocy;
     int x0 = 0, x1 = 0, y0 = 0, y1 = 0;
     bool changed = true;
-    int status = R_OK;
+    int status = R_OK, nins = 0;
     const int max_phase = S.xsize + S.ysize + 8;
 
-    // one candidate per lane (have): classify all, then insert the conflicting ones one at a
-    // time (the others re-test against each new ring)
     // one candidate per lane (have): classify all, then insert the conflicting ones one at a
     // time, nearest first (a near candidate is the likelier Delaunay neighbour, and inserting
     // it shrinks the circles the farther ones conflict with); after each insertion the others
@@ -163,6 +212,7 @@ __device__ int coop_run(B &b, const int lane)
                 break;
             }
             changed = true;
+            ++nins;
             const bool again = ((want >> lane) & 1u) && lane != leader;
             if (again) {
                 int s, e, c, ns;
@@ -184,9 +234,10 @@ __device__ int coop_run(B &b, const int lane)
         const int w = xb - xa + 1, ncell = w * (yb - ya + 1);
         for (int cb = 0; cb < ncell && status == R_OK; cb += 32) {
             const int ci = cb + lane;
-            int start = 0, cnt = 0;
+            int start = 0, cnt = 0, rx = 0, ry = 0;
             if (ci < ncell) {
-                const int rx = xa + ci % w, ry = ya + ci / w;
+                rx = xa + ci % w;
+                ry = ya + ci / w;
                 const int cx = wrapi(b.ocx + rx, S.xsize), cy = wrapi(b.ocy + ry, S.ysize);
                 const int blk = S.block_base + (cy >> BLOCK_SHIFT) * S.bxsize + (cx >> BLOCK_SHIFT);
                 if (__ldg(&A.bcount[blk]) != 0 && (!prune || b.cell_reached(rx, ry, fx, fy))) {
@@ -196,21 +247,51 @@ __device__ int coop_run(B &b, const int lane)
                     b.ctr.add_cells();
                 }
             }
-            int incl = cnt;
-            for (int o = 1; o < 32; o <<= 1) {
-                int v = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += v;
-            }
-            const int total = __shfl_sync(0xffffffffu, incl, 31), excl = incl - cnt;
-            for (int j0 = 0; j0 < total && status == R_OK; j0 += 32) {
-                const int j = j0 + lane;
-                int o = 0;   // the last lane whose cell range starts at or before j
+            // the cells' candidates 32 at a time; after a chunk that changed the ring, the
+            // cells with candidates left are tested against the shrunken circles again
+            while (status == R_OK) {
+                int incl = cnt;
+                for (int o = 1; o < 32; o <<= 1) {
+                    int v = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += v;
+                }
+                const int total = __shfl_sync(0xffffffffu, incl, 31), excl = incl - cnt;
+                if (total == 0) break;
+                int o = 0;   // the last lane whose cell range starts at or before this lane's slot
                 for (int step = 16; step > 0; step >>= 1) {
                     int e = __shfl_sync(0xffffffffu, excl, o + step);
-                    if (e <= j) o += step;
+                    if (e <= lane) o += step;
                 }
-                const int sl = __shfl_sync(0xffffffffu, start, o) + j - __shfl_sync(0xffffffffu, excl, o);
-                settle(sl, j < total);
+                const int sl = __shfl_sync(0xffffffffu, start, o) + lane - __shfl_sync(0xffffffffu, excl, o);
+                const int m_before = nins;
+                settle(sl, lane < total);
+                const int used = min(cnt, max(0, 32 - excl));
+                start += used;
+                cnt -= used;
+                if (prune && nins != m_before && cnt > 0 && !b.cell_reached(rx, ry, fx, fy)) cnt = 0;
+            }
+        }
+    };
+
+    // the cells [xa, xb] x [ya, yb] of strip q as 8 x 8-cell tiles (see strip_tile), one per
+    // lane; the live ones are scanned cell by cell
+    auto scan_tiles = [&](int xa, int xb, int ya, int yb, int q) {
+        const int ntile = (((xb - xa) >> BLOCK_SHIFT) + 1) * (((yb - ya) >> BLOCK_SHIFT) + 1);
+        for (int tb = 0; tb < ntile && status == R_OK; tb += 32) {
+            const int ti = tb + lane;
+            int ta = 0, tbx = -1, tc = 0, td = -1;
+            bool live = false;
+            if (ti < ntile) {
+                strip_tile(ti, q, xa, xb, ya, yb, BLOCK_SHIFT, ta, tbx, tc, td);
+                live = occupied(A.bcount, S.block_base, S.bxsize, BLOCK_SHIFT, S, b.ocx, b.ocy, ta, tbx, tc, td) &&
+                       b.rect_reached(ta, tbx, tc, td, fx, fy);
+            }
+            unsigned todo = __ballot_sync(0xffffffffu, live);
+            while (todo && status == R_OK) {
+                const int src = __ffs(todo) - 1;
+                todo &= todo - 1;
+                scan_cells(__shfl_sync(0xffffffffu, ta, src), __shfl_sync(0xffffffffu, tbx, src),
+                           __shfl_sync(0xffffffffu, tc, src), __shfl_sync(0xffffffffu, td, src), true);
             }
         }
     };
@@ -254,41 +335,31 @@ __device__ int coop_run(B &b, const int lane)
                 scan_cells(sxa[q], sxb[q], sya[q], syb[q], phase >= 2);
                 continue;
             }
-            // a large strip: 8 x 8 tiles first, one per lane; a tile is scanned cell by cell
-            // only when one of the occupancy blocks it touches holds points and its rectangle
-            // meets a current circle (empty space costs one test per tile, not per cell)
-            const int tw = (sw + 7) >> 3, th = (sh + 7) >> 3, ntile = tw * th;
+            // a large strip: tiles first, one per lane, nearest first; a tile is opened only
+            // when an occupancy block it touches holds points and its rectangle meets a current
+            // circle (empty space costs one test per tile, not per cell).  A strip of more than
+            // 64 tiles of 8 x 8 cells is cut into 64 x 64-cell tiles first, judged by the
+            // super-block occupancy, and only those are opened into 8 x 8-cell tiles.
+            if ((((sw - 1) >> BLOCK_SHIFT) + 1) * (((sh - 1) >> BLOCK_SHIFT) + 1) <= 64) {
+                scan_tiles(sxa[q], sxb[q], sya[q], syb[q], q);
+                continue;
+            }
+            const int ntile = (((sw - 1) >> SBLOCK_SHIFT) + 1) * (((sh - 1) >> SBLOCK_SHIFT) + 1);
             for (int tb = 0; tb < ntile && status == R_OK; tb += 32) {
                 const int ti = tb + lane;
                 int ta = 0, tbx = -1, tc = 0, td = -1;
                 bool live = false;
                 if (ti < ntile) {
-                    // nearest tiles first: the left strip from its right edge, the bottom strip
-                    // from its top edge (the others start next to the old rectangle already)
-                    const int ix = q == 0 ? tw - 1 - ti % tw : ti % tw, iy = q == 2 ? th - 1 - ti / tw : ti / tw;
-                    ta = sxa[q] + ix * 8;
-                    tbx = min(ta + 7, sxb[q]);
-                    tc = sya[q] + iy * 8;
-                    td = min(tc + 7, syb[q]);
-                    // occupancy of the (up to 3 x 3) blocks the tile touches
-                    for (int xs = ta; xs <= tbx && !live;) {
-                        const int ax = wrapi(b.ocx + xs, S.xsize), bx = ax >> BLOCK_SHIFT;
-                        const int xe = xs + min((bx + 1) << BLOCK_SHIFT, S.xsize) - ax;   // next block's first x
-                        for (int ys = tc; ys <= td && !live;) {
-                            const int ay = wrapi(b.ocy + ys, S.ysize), by = ay >> BLOCK_SHIFT;
-                            live = __ldg(&A.bcount[S.block_base + by * S.bxsize + bx]) != 0;
-                            ys += min((by + 1) << BLOCK_SHIFT, S.ysize) - ay;
-                        }
-                        xs = xe;
-                    }
-                    live = live && b.rect_reached(ta, tbx, tc, td, fx, fy);
+                    strip_tile(ti, q, sxa[q], sxb[q], sya[q], syb[q], SBLOCK_SHIFT, ta, tbx, tc, td);
+                    live = occupied(A.bcount, S.sblock_base, S.sbxsize, SBLOCK_SHIFT, S, b.ocx, b.ocy, ta, tbx, tc, td) &&
+                           b.rect_reached(ta, tbx, tc, td, fx, fy);
                 }
                 unsigned todo = __ballot_sync(0xffffffffu, live);
                 while (todo && status == R_OK) {
                     const int src = __ffs(todo) - 1;
                     todo &= todo - 1;
-                    scan_cells(__shfl_sync(0xffffffffu, ta, src), __shfl_sync(0xffffffffu, tbx, src),
-                               __shfl_sync(0xffffffffu, tc, src), __shfl_sync(0xffffffffu, td, src), true);
+                    scan_tiles(__shfl_sync(0xffffffffu, ta, src), __shfl_sync(0xffffffffu, tbx, src),
+                               __shfl_sync(0xffffffffu, tc, src), __shfl_sync(0xffffffffu, td, src), q);
                 }
             }
         }
