@@ -365,6 +365,8 @@ BinArgs bin_args(dgt_context *c, const double *pts)
     a.block_sums = c->bsum.as<int>();
     a.deterministic = c->deterministic;
     a.cond = nullptr;
+    a.num_sets = c->num_sets;
+    a.total_blocks = c->total_blocks;
     return a;
 }
 

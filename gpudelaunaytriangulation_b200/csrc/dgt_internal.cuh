@@ -192,6 +192,8 @@ struct BinArgs {
     int *block_sums;
     int deterministic;
     const int *cond;    // null: bin; else bin only when *cond != 0 (device-side decision)
+    int num_sets;       // entries of sets
+    int total_blocks;   // entries of bcount (blocks and super-blocks of every set)
 };
 
 struct RingArgs {

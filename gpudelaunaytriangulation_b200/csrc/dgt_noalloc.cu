@@ -178,6 +178,8 @@ extern "C" int dgt_global_triangulation_noalloc(const double *d_points, int n, d
     b.bcount = reinterpret_cast<int *>(base + OFF_BCOUNT);
     b.deterministic = 1;
     b.cond = nullptr;
+    b.num_sets = 1;
+    b.total_blocks = blocks;
     if (launch_bin_st(b, d_st, s) != cudaSuccess) return DGT_ERR_CUDA;
 
     RingArgs r;

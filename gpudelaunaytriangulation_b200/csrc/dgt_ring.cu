@@ -88,12 +88,13 @@ __global__ void __launch_bounds__(BLOCK) k_build(RingArgs A)
 // float32 nor float64 decides, and scans longer than the work budget (typically on the rim of
 // dense clusters, where the circles reach over large, partly empty and partly dense regions)
 // -- are rebuilt by a whole warp.  The 32 lanes share one ring in shared memory (float32
-// filter, float64 recheck, exact residue, 64 entries), take 32 new cells at a time (dropping empty occupancy
-// blocks and cells that no current circle reaches) and 32 candidates at a time.  One lane inserts; lanes whose
-// candidates conflicted test them again against the new ring (a candidate outside every
-// circle stays outside, see cell_reached).  The scanned rectangle grows one cell per side
-// while the ring keeps changing, by half its extent while virtual corners are left, and
-// straight to the circles' cells once a layer changed nothing.
+// filter, float64 recheck, exact residue, 64 entries), take 32 new cells at a time (dropping
+// cells that no current circle reaches; wide strips are first judged as tiles of 8 x 8 and
+// 64 x 64 cells against the two occupancy levels) and 32 candidates at a time.  One lane
+// inserts; lanes whose candidates conflicted test them again against the new ring (a
+// candidate outside every circle stays outside, see cell_reached).  The scanned rectangle
+// grows one cell per side while the ring keeps changing, by half its extent while virtual
+// corners are left, and straight to the circles' cells once a layer changed nothing.
 constexpr int WARP_KERNEL_CAP = 64;
 constexpr int WARP_KERNEL_WARPS = 4;   // warps (points) per block
 
@@ -151,20 +152,31 @@ __device__ __forceinline__ void strip_tile(int ti, int q, int xa, int xb, int ya
 }
 
 // Whether any occupancy entry of 2^sh x 2^sh cells (row-major from `base`, `row` per row)
-// that the cells [xa, xb] x [ya, yb] relative to (ocx, ocy), wrapped, touch holds points
+// that the cells [xa, xb] x [ya, yb] relative to (ocx, ocy), wrapped, touch holds points.  A
+// span of at most 2^sh cells touches at most three entries per axis (two, plus the grid's
+// partial last entry where it wraps); the loads are independent of each other.
 __device__ __forceinline__ bool occupied(const int *cnt, int base, int row, int sh, const SetDesc &S, int ocx, int ocy,
                                          int xa, int xb, int ya, int yb)
 {
-    for (int xs = xa; xs <= xb;) {
-        const int ax = wrapi(ocx + xs, S.xsize), bx = ax >> sh;
-        for (int ys = ya; ys <= yb;) {
-            const int ay = wrapi(ocy + ys, S.ysize), by = ay >> sh;
-            if (__ldg(&cnt[base + by * row + bx]) != 0) return true;
-            ys += min((by + 1) << sh, S.ysize) - ay;
-        }
-        xs += min((bx + 1) << sh, S.xsize) - ax;
+    int ex[3], ey[3], nx = 0, ny = 0, xs = xa, ys = ya;
+    for (; xs <= xb && nx < 3; ++nx) {
+        const int ax = wrapi(ocx + xs, S.xsize);
+        ex[nx] = ax >> sh;
+        xs += min((ex[nx] + 1) << sh, S.xsize) - ax;
     }
-    return false;
+    for (; ys <= yb && ny < 3; ++ny) {
+        const int ay = wrapi(ocy + ys, S.ysize);
+        ey[ny] = ay >> sh;
+        ys += min((ey[ny] + 1) << sh, S.ysize) - ay;
+    }
+    if (xs <= xb || ys <= yb) return true;   // wider than 2^sh cells: judged occupied
+    int acc = 0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+            if (i < nx && j < ny) acc |= __ldg(&cnt[base + ey[j] * row + ex[i]]);
+    return acc != 0;
 }
 
 template <class B>
@@ -228,8 +240,8 @@ __device__ int coop_run(B &b, const int lane)
         }
     };
     // every candidate of the cells [xa, xb] x [ya, yb] (relative to the own cell): 32 cells
-    // at a time, one per lane (empty occupancy blocks dropped, and with `prune` the cells no
-    // current circle reaches), then their candidates 32 at a time
+    // at a time, one per lane (with `prune`, the cells no current circle reaches are dropped),
+    // then their candidates 32 at a time
     auto scan_cells = [&](int xa, int xb, int ya, int yb, bool prune) {
         const int w = xb - xa + 1, ncell = w * (yb - ya + 1);
         for (int cb = 0; cb < ncell && status == R_OK; cb += 32) {
@@ -239,13 +251,11 @@ __device__ int coop_run(B &b, const int lane)
                 rx = xa + ci % w;
                 ry = ya + ci / w;
                 const int cx = wrapi(b.ocx + rx, S.xsize), cy = wrapi(b.ocy + ry, S.ysize);
-                const int blk = S.block_base + (cy >> BLOCK_SHIFT) * S.bxsize + (cx >> BLOCK_SHIFT);
-                if (__ldg(&A.bcount[blk]) != 0 && (!prune || b.cell_reached(rx, ry, fx, fy))) {
-                    const int c = S.cell_base + cy * S.xsize + cx;
-                    start = __ldg(&A.cstart[c]);
-                    cnt = __ldg(&A.cstart[c + 1]) - start;
-                    b.ctr.add_cells();
-                }
+                const int c = S.cell_base + cy * S.xsize + cx;
+                start = __ldg(&A.cstart[c]);
+                cnt = __ldg(&A.cstart[c + 1]) - start;
+                if (cnt > 0 && prune && !b.cell_reached(rx, ry, fx, fy)) cnt = 0;
+                if (cnt > 0) b.ctr.add_cells();
             }
             // the cells' candidates 32 at a time; after a chunk that changed the ring, the
             // cells with candidates left are tested against the shrunken circles again
