@@ -685,8 +685,8 @@ def run_profile_case(args):
     triangulations of n seeded uniform points at unit density (build, repair), or in a
     general 60-degree box at unit density (hex); with `repair`, one test-and-repair after a
     sigma = 0.02 displacement.  Launch order per triangulation: 6 binning kernels, k_build,
-    k_build_warp.  `md`: the 256-set ensemble, one build, then `--reps` MD steps.  Prints the
-    counters of the calls."""
+    k_build_warp.  `md`: the 256-set ensemble, one build, then `--reps` MD steps.  `mixture`:
+    the 1M-point 64-cluster mixture at its tuned settings.  Prints the counters of the calls."""
     import math
 
     import torch
@@ -710,6 +710,24 @@ def run_profile_case(args):
                 b.mdStep(P, tri, nn, 0.01, seed=8, rounds=4, stream=stream)
             stream.synchronize()
         print(json.dumps({"md": b.stats()}))
+        return 0
+    if args.profile == "mixture":
+        # the clustered workload of the mixture_1m_fp32 measurement (1,048,576 points, 64
+        # Gaussian clusters of std 2 in a 1024 box) at the settings the autotuner picks for it
+        # (cell edge 0.25 of the mean spacing, work budget 512, 14-entry ring at 32 threads per
+        # block), `--reps` global triangulations
+        pts, L = W.gaussian_mixture(1 << 20, components=64, sigma=2.0, L=1024.0, seed=5)
+        n = len(pts)
+        d = DelaunayGPU(n, 24, 0.25 * L / math.sqrt(n), (L, L))
+        d.setKernelShape(3)
+        d.setWorkBudget(512)
+        d.setTiming(True)
+        P = torch.from_numpy(pts).cuda()
+        tri = torch.zeros(24 * n, dtype=torch.int32, device="cuda")
+        nn = torch.zeros(n, dtype=torch.int32, device="cuda")
+        for _ in range(args.reps):
+            tri, nn = d.globalDelaunayTriangulation(P, tri, nn)
+        print(json.dumps({"mixture": d.stats(), "build_ms": d.phaseTimes()}))
         return 0
     n = args.n or (1 << 20)
     L = math.sqrt(n)
@@ -752,7 +770,7 @@ def main():
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble MD measurement")
     ap.add_argument("--no-configs", action="store_true", help="skip the other workload families")
     ap.add_argument("--no-reference-gpu", action="store_true", help="skip timing the reference's own CUDA kernels")
-    ap.add_argument("--profile", choices=["build", "repair", "hex", "md"], default=None,
+    ap.add_argument("--profile", choices=["build", "repair", "hex", "md", "mixture"], default=None,
                     help="profiling case for Nsight Compute: a fixed, small sequence of calls (no timing)")
     ap.add_argument("--reps", type=int, default=2, help="global triangulations per --profile run")
     args = ap.parse_args()

@@ -395,6 +395,41 @@ def test_batched_sets_match_per_set_oracle():
         assert np.array_equal(O.canonical(ts, k[lo:hi])[:, :16], O.canonical(ref.tri, ref.nn)[:, :16])
 
 
+def test_batched_clustered_sets_through_warp_kernel_match_oracle():
+    # clustered sets of different sizes and boxes in one batch, at a quarter of each set's
+    # mean spacing and a small work budget: many points go to the warp-per-point kernel, whose
+    # scans of the voids between clusters cross strips of thousands of cells and so are judged
+    # on both occupancy levels (8 x 8-cell blocks and 64 x 64-cell super-blocks, the latter
+    # filled per set from the block counts)
+    from gpudelaunaytriangulation_b200.delaunay import DelaunayBatch
+
+    # clusters ~32 units apart, as in the 1M-point workload (wider voids let circles pass half
+    # the box, where the reference's minimum-image search itself fails)
+    specs = [(32768, 32, 181.0, 33), (24000, 24, 156.0, 34), (32768, 32, 181.0, 36)]
+    sets = [W.gaussian_mixture(n, components=c, sigma=2.0, L=L, seed=s) for n, c, L, s in specs]
+    pts = np.concatenate([p for p, _ in sets], axis=0)
+    sizes = np.array([len(p) for p, _ in sets])
+    boxes = np.array([[L, L] for _, L in sets])
+    b = DelaunayBatch(sizes, boxes, 32, 0.25)
+    b.setWorkBudget(64)
+    P = torch.from_numpy(pts).cuda()
+    tri = torch.zeros(32 * len(pts), dtype=torch.int32, device="cuda")
+    nn = torch.zeros(len(pts), dtype=torch.int32, device="cuda")
+    b.globalDelaunayTriangulation(P, tri, nn)
+    st = b.stats()
+    assert st["error_flags"] == 0 and st["heavy_points"] > 1000, st
+    t, k = host(tri, nn)
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    for s in range(len(sizes)):
+        lo, hi = off[s], off[s + 1]
+        ref = O.restated_global(pts[lo:hi], boxes[s][0], boxes[s][1], 1.0, 32)
+        ts = t[lo:hi].copy()
+        ts[np.arange(ts.shape[1])[None, :] < k[lo:hi, None]] -= lo
+        assert np.array_equal(k[lo:hi], ref.nn), s
+        assert np.array_equal(O.canonical(ts, k[lo:hi]), O.canonical(ref.tri, ref.nn)[:, :32]), s
+    b.close()
+
+
 def test_million_points_properties():
     n = 1_000_000
     L = 1000.0
