@@ -17,7 +17,7 @@ INCLUDE = os.path.join(ROOT, "include")
 LIBDIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(LIBDIR, "libdgt.so")
 SOURCES = ["dgt_bin.cu", "dgt_ring.cu", "dgt_group.cu", "dgt_flip.cu", "dgt_validate.cu", "dgt_api.cu",
-           "dgt_noalloc.cu"]
+           "dgt_noalloc.cu", "dgt_hilbert.cu"]
 HEADERS = ["dgt_internal.cuh", "dgt_predicates.cuh", "dgt_rowreg.cuh", "dgt_builder.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -87,7 +87,7 @@ struct dgt_context {
     int total_cells = 0;
     int total_blocks = 0;
     DevBuf d_sets, d_set_of, ccount, cstart, cell_of, rank, sidx, slot_of, spos, bsum, mark, list0, list1,
-        defer_list, st, ctl, bcount, claim, flip0, flip1, quad, vcount;
+        defer_list, st, ctl, bcount, claim, flip0, flip1, quad, vcount, hsets, hcount, hstart, hsum, hbucket, hrank;
     DevStatus *h_st = nullptr;
     cudaStream_t last_stream = nullptr;
     bool stats_valid = false;
@@ -616,7 +616,8 @@ void dgt_destroy(dgt_context *c)
     if (!c) return;
     DevBuf *bufs[] = { &c->d_sets, &c->d_set_of, &c->ccount, &c->cstart, &c->cell_of, &c->rank, &c->sidx,
                        &c->slot_of, &c->spos, &c->bsum, &c->mark, &c->list0, &c->list1, &c->defer_list,
-                       &c->st, &c->ctl, &c->bcount, &c->claim, &c->flip0, &c->flip1, &c->quad, &c->vcount };
+                       &c->st, &c->ctl, &c->bcount, &c->claim, &c->flip0, &c->flip1, &c->quad, &c->vcount,
+                       &c->hsets, &c->hcount, &c->hstart, &c->hsum, &c->hbucket, &c->hrank };
     for (DevBuf *b : bufs) b->release();
     if (c->h_st) cudaFreeHost(c->h_st);
     for (int p = 0; p < DGT_NUM_PHASES; ++p)
@@ -1110,6 +1111,54 @@ int dgt_get_cell_order(dgt_context *c, int *d_order, void *stream)
     if (!d_order || !c->binned) return DGT_ERR_INVALID_ARGUMENT;
     DGT_TRY(cudaMemcpyAsync(d_order, c->sidx.p, sizeof(int) * (size_t)c->n, cudaMemcpyDeviceToDevice,
                             (cudaStream_t)stream));
+    return DGT_OK;
+}
+
+int dgt_get_hilbert_order(dgt_context *c, const double *d_points, int *d_order, void *stream)
+{
+    if (!c) return DGT_ERR_INVALID_ARGUMENT;
+    if (c->n == 0) return DGT_OK;
+    if (!d_points || !d_order) return DGT_ERR_INVALID_ARGUMENT;
+    // per set: the smallest 2^k x 2^k grid with at least one square per point (k <= 15),
+    // its scale over the box (a general box: over the fractional frame) and its first key
+    std::vector<HilbertSet> hs((size_t)c->num_sets);
+    long long buckets = 0;
+    for (int s = 0; s < c->num_sets; ++s) {
+        int k = 1;
+        while (k < 15 && (1LL << (2 * k)) < (long long)c->sizes[s]) ++k;
+        const double g = (double)(1 << k);
+        hs[s].k = k;
+        hs[s].base = (int)buckets;
+        hs[s].sx = c->general ? g : g / c->boxes[2 * s];
+        hs[s].sy = c->general ? g : g / c->boxes[2 * s + 1];
+        buckets += 1LL << (2 * k);
+        if (buckets >= (1LL << 31) - 1) return DGT_ERR_INVALID_ARGUMENT;
+    }
+    const int nb = (int)buckets;
+    cudaStream_t st = (cudaStream_t)stream;
+    DGT_TRY(c->hsets.ensure(sizeof(HilbertSet) * hs.size()));
+    DGT_TRY(c->hcount.ensure(sizeof(int) * ((size_t)nb + 1)));
+    DGT_TRY(c->hstart.ensure(sizeof(int) * ((size_t)nb + 1)));
+    DGT_TRY(c->hsum.ensure(sizeof(int) * ((size_t)scan_block_count(nb + 1) + 1)));
+    DGT_TRY(c->hbucket.ensure(sizeof(int) * (size_t)c->n));
+    DGT_TRY(c->hrank.ensure(sizeof(int) * (size_t)c->n));
+    DGT_TRY(cudaMemcpyAsync(c->hsets.p, hs.data(), sizeof(HilbertSet) * hs.size(), cudaMemcpyHostToDevice, st));
+    HilbertArgs a;
+    a.pos = reinterpret_cast<const double2 *>(d_points);
+    a.n = c->n;
+    a.sets = c->d_sets.as<SetDesc>();
+    a.set_of = c->batch ? c->d_set_of.as<int>() : nullptr;
+    a.hsets = c->hsets.as<HilbertSet>();
+    a.buckets = nb;
+    a.hcount = c->hcount.as<int>();
+    a.hstart = c->hstart.as<int>();
+    a.bsum = c->hsum.as<int>();
+    a.hbucket = c->hbucket.as<int>();
+    a.hrank = c->hrank.as<int>();
+    a.order = d_order;
+    DGT_TRY(launch_hilbert_order(a, st));
+    // the host copy of the descriptors must outlive the transfer
+    DGT_TRY(cudaStreamSynchronize(st));
     return DGT_OK;
 }
 

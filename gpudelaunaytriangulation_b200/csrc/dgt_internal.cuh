@@ -303,6 +303,28 @@ cudaError_t launch_clear_counts(int *ccount, int ncell, int *bcount, int nblock,
 constexpr float MAX_SKIN_CELLS = 0.5f;
 cudaError_t launch_scan(const int *in, int n, int *bsum, int *out, cudaStream_t s);
 int scan_block_count(int n);
+
+// Hilbert order of the points (dgt_hilbert.cu): per set, the curve's 2^k x 2^k grid, the
+// scale from a position (rectangular box) or a fractional coordinate (general box) to grid
+// squares, and the set's first key
+struct HilbertSet {
+    double sx, sy;
+    int k, base;
+};
+struct HilbertArgs {
+    const double2 *pos;
+    int n;
+    const SetDesc *sets;
+    const int *set_of;
+    const HilbertSet *hsets;
+    int buckets;       // keys of all sets
+    int *hcount;       // buckets + 1 (zeroed by the launcher)
+    int *hstart;       // buckets + 1
+    int *bsum;         // scan_block_count(buckets + 1)
+    int *hbucket, *hrank;   // n each
+    int *order;        // n: the result
+};
+cudaError_t launch_hilbert_order(const HilbertArgs &a, cudaStream_t s);
 constexpr int KERNEL_SHAPES = 7;
 int kernel_shape_cap(int shape);
 int kernel_shape_block(int shape);

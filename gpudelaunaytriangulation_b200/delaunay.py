@@ -321,6 +321,18 @@ class DelaunayGPU:
             _nat.check(self._L.dgt_get_cell_order(self._h, _ptr(out), _stream_ptr(stream)), "dgt_get_cell_order")
         return out
 
+    def hilbertOrder(self, points: torch.Tensor, stream=None) -> torch.Tensor:
+        """Indices of the points along a Hilbert curve over each set's box (int32, on the
+        device; the reference's hilbertSortArray pre-pass, triangulation.cpp:63-88):
+        renumbering the points in this order puts Delaunay neighbours at nearby indices."""
+        n = self.Ncells
+        _check_points(points, n)
+        out = torch.empty(n, dtype=torch.int32, device=points.device)
+        if n:
+            _nat.check(self._L.dgt_get_hilbert_order(self._h, _ptr(points), _ptr(out), _stream_ptr(stream)),
+                       "dgt_get_hilbert_order")
+        return out
+
     def setFlipRepair(self, on: bool):
         """Test-and-repair by Lawson flips first (default) or by rebuilding every flagged point."""
         _nat.check(self._L.dgt_set_flip_repair(self._h, int(bool(on))), "dgt_set_flip_repair")

@@ -192,6 +192,16 @@ int dgt_validate(dgt_context *ctx, const double *d_points, const int *d_tri, con
  * the context first (DGT_ERR_INVALID_ARGUMENT otherwise); d_order is int[n] on the device. */
 int dgt_get_cell_order(dgt_context *ctx, int *d_order, void *stream);
 
+/* Hilbert-curve order of d_points (replaces the reference's hilbertSortArray pre-pass,
+ * triangulation.cpp:63-88 over xy2d, src/utilities/hilbert_curve.cpp:229, which sorts on the
+ * host along a curve of unit squares): d_order[k] = index of the k-th point along a Hilbert
+ * curve laid over each set's box (a general box: over its fractional frame) with a 2^k x 2^k
+ * grid, the smallest with at least one square per point (k <= 15); points of one square by
+ * index; batched contexts set by set.  Needs no earlier call; d_points double2[n] and d_order
+ * int[n] on the device.  Allocates its scratch on first use (16 to 40 bytes per point, with
+ * the grid) and synchronises `stream` before it returns. */
+int dgt_get_hilbert_order(dgt_context *ctx, const double *d_points, int *d_order, void *stream);
+
 /* 1: record CUDA events around each phase of every call (on the call's stream). */
 int dgt_set_timing(dgt_context *ctx, int on);
 /* Milliseconds per phase of the last call (DGT_NUM_PHASES values, -1 for phases the call did

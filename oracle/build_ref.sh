@@ -5,7 +5,8 @@
 #
 # Sources used (paths inside the reference project):
 #   src/model/DelaunayGPU.cu, src/model/DelaunayGPU.cpp,
-#   src/utilities/cellListGPU.cu, src/utilities/cellListGPU.cpp, src/utilities/utilities.cu
+#   src/utilities/cellListGPU.cu, src/utilities/cellListGPU.cpp, src/utilities/utilities.cu,
+#   src/utilities/hilbert_curve.cpp
 # The reference's CMake build is not used (it pins gcc-6 and sm_35, CMakeLists.txt:2-18);
 # -DNVCC is needed so HOSTDEVICE keeps __device__ (src/utilities/indexer.h:20-24) and the
 # nvtx3 include dir because inc/std_include.h:41 includes nvToolsExt.h.
@@ -30,8 +31,10 @@ nvcc $NVFLAGS $INC -c "$REF/src/utilities/cellListGPU.cu"   -o "$OUT/obj/cellLis
 nvcc $NVFLAGS $INC -c "$REF/src/utilities/utilities.cu"     -o "$OUT/obj/utilities_cu.o"
 g++ $CXXFLAGS $INC -c "$REF/src/model/DelaunayGPU.cpp"      -o "$OUT/obj/DelaunayGPU_cpp.o"
 g++ $CXXFLAGS $INC -c "$REF/src/utilities/cellListGPU.cpp"  -o "$OUT/obj/cellListGPU_cpp.o"
+g++ $CXXFLAGS $INC -c "$REF/src/utilities/hilbert_curve.cpp" -o "$OUT/obj/hilbert_curve_cpp.o"
 nvcc $NVFLAGS $INC -c "$HERE/ref_harness.cu"                -o "$OUT/obj/ref_harness.o"
 nvcc -shared -gencode arch=compute_100a,code=sm_100a -Xcompiler -fopenmp -o "$OUT/libdgtref.so" \
     "$OUT/obj/DelaunayGPU_cu.o" "$OUT/obj/cellListGPU_cu.o" "$OUT/obj/utilities_cu.o" \
-    "$OUT/obj/DelaunayGPU_cpp.o" "$OUT/obj/cellListGPU_cpp.o" "$OUT/obj/ref_harness.o" \
+    "$OUT/obj/DelaunayGPU_cpp.o" "$OUT/obj/cellListGPU_cpp.o" "$OUT/obj/hilbert_curve_cpp.o" \
+    "$OUT/obj/ref_harness.o" \
     -L"$CUDA/lib64" -lcudart -lgomp

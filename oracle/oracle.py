@@ -152,6 +152,8 @@ def ref_lib():
         R.ref_gpu_fetch.argtypes = [ctypes.c_void_p, _P_I, _P_I, ctypes.c_int]
         R.ref_gpu_destroy.restype = None
         R.ref_gpu_destroy.argtypes = [ctypes.c_void_p]
+        R.ref_xy2d.restype = ctypes.c_int
+        R.ref_xy2d.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
         _ref = R
     return _ref
 
@@ -387,6 +389,61 @@ def reduce_basis(box):
     bx = np.array(box, dtype=np.float64)
     lib().orc_reduce_basis(_pd(bx))
     return tuple(float(v) for v in bx)
+
+
+def hilbert_index(k, x, y):
+    """Hilbert-curve index of grid squares (x, y) of a 2^k x 2^k grid (integer arrays): the
+    standard conversion the reference's xy2d performs (src/utilities/hilbert_curve.cpp:229,
+    with its quadrant rotation rot, :137), restated level by level from the coarsest."""
+    x = np.asarray(x, dtype=np.int64).copy()
+    y = np.asarray(y, dtype=np.int64).copy()
+    d = np.zeros(np.broadcast(x, y).shape, dtype=np.int64)
+    for lv in range(k - 1, -1, -1):
+        s = 1 << lv
+        rx = (x >> lv) & 1
+        ry = (y >> lv) & 1
+        d += s * s * ((3 * rx) ^ ry)
+        x &= s - 1
+        y &= s - 1
+        refl = (ry == 0) & (rx == 1)
+        x = np.where(refl, s - 1 - x, x)
+        y = np.where(refl, s - 1 - y, y)
+        swap = ry == 0
+        x, y = np.where(swap, y, x), np.where(swap, x, y)
+    return d
+
+
+def reference_xy2d(m, x, y) -> int:
+    """The reference's own xy2d (oracle/_ref), or None when it was not built."""
+    R = ref_lib()
+    return None if R is None else int(R.ref_xy2d(int(m), int(x), int(y)))
+
+
+def hilbert_order(points, sizes, boxes):
+    """Order of the points along a Hilbert curve over each set's rectangular box, set by set:
+    a 2^k x 2^k grid per set (the smallest with 4^k >= its points, 1 <= k <= 15), square
+    (floor(x * (2^k / Lx)), floor(y * (2^k / Ly))) clamped to the grid, points sorted by
+    square index then by point index."""
+    points = np.asarray(points, dtype=np.float64)
+    out, off = [], 0
+    for n, (Lx, Ly) in zip(sizes, boxes):
+        n = int(n)
+        k = 1
+        while k < 15 and (1 << (2 * k)) < n:
+            k += 1
+        g = 1 << k
+        p = points[off:off + n]
+
+        def square(u):
+            q = np.zeros(len(u), dtype=np.int64)
+            ok = u >= 0.0
+            q[ok] = np.where(u[ok] < g, np.floor(u[ok]), g - 1).astype(np.int64)
+            return q
+
+        key = hilbert_index(k, square(p[:, 0] * (g / Lx)), square(p[:, 1] * (g / Ly)))
+        out.append(np.lexsort((np.arange(n), key)) + off)
+        off += n
+    return np.concatenate(out) if out else np.zeros(0, dtype=np.int64)
 
 
 def canonical(tri, nn):

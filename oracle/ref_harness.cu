@@ -49,6 +49,7 @@
 #include "periodicBoundaries.h"
 #include "DelaunayGPU.cuh"
 #include "DelaunayGPU.h"
+#include "hilbert_curve.hpp"
 
 namespace {
 
@@ -411,5 +412,9 @@ void ref_gpu_destroy(void *h)
     delete r->del;
     delete r;
 }
+
+/* The reference's Hilbert index of square (x, y) of a 2^m x 2^m grid
+   (src/utilities/hilbert_curve.cpp:229; the key of its hilbertSortArray pre-pass). */
+int ref_xy2d(int m, int x, int y) { return xy2d(m, x, y); }
 
 }  // extern "C"

@@ -163,3 +163,31 @@ def test_reference_seed_pass_guard_measures_polygons():
     mx = O.reference_seed_max(pts, L, L, 1.0, 64)
     assert 4 <= mx <= 12
     assert O.reference_seed_max(pts, L, L, 1.0, mx) == -1
+
+
+@pytest.mark.skipif(O.ref_lib() is None, reason="oracle/_ref not built (reference sources absent)")
+def test_hilbert_index_matches_reference_xy2d():
+    # the restated curve index equals the reference's own xy2d (hilbert_curve.cpp:229) at every
+    # grid order the device ordering uses
+    rng = np.random.default_rng(5)
+    for m in range(1, 16):
+        g = 1 << m
+        xs, ys = rng.integers(0, g, 300), rng.integers(0, g, 300)
+        mine = O.hilbert_index(m, xs, ys)
+        ref = np.array([O.reference_xy2d(m, a, b) for a, b in zip(xs, ys)])
+        assert np.array_equal(mine, ref), m
+
+
+def test_hilbert_index_is_a_continuous_curve():
+    # known answers of the curve: on a 2^m grid the index is a bijection onto [0, 4^m), and
+    # squares with consecutive indices share an edge
+    for m in (1, 2, 3, 5):
+        g = 1 << m
+        x, y = np.meshgrid(np.arange(g), np.arange(g))
+        d = O.hilbert_index(m, x.ravel(), y.ravel())
+        assert np.array_equal(np.sort(d), np.arange(g * g))
+        at = np.argsort(d)
+        step = np.abs(np.diff(x.ravel()[at])) + np.abs(np.diff(y.ravel()[at]))
+        assert (step == 1).all(), m
+    # the first-order curve: (0,0) -> (0,1) -> (1,1) -> (1,0)
+    assert O.hilbert_index(1, [0, 0, 1, 1], [0, 1, 1, 0]).tolist() == [0, 1, 2, 3]
