@@ -34,7 +34,7 @@ EXPORTED = [
     "dgt_md_graph_launch", "dgt_md_graph_destroy", "dgt_clear_flags", "dgt_set_kernel_shape",
     "dgt_get_tuning", "dgt_autotune", "dgt_set_work_budget", "dgt_set_flip_repair",
     "dgt_validate", "dgt_get_cell_order", "dgt_set_box_general", "dgt_get_box", "dgt_create_batch_general",
-    "dgt_set_graph_flip_rounds", "dgt_get_hilbert_order",
+    "dgt_set_graph_flip_rounds", "dgt_get_hilbert_order", "dgt_set_deferred_overlap",
 ]
 STEP_AUTO = 0xFFFFFFFFFFFFFFFF
 NOALLOC_MAX_POINTS = 65536
@@ -100,6 +100,8 @@ class TuneResult(ctypes.Structure):
         ("default_ms", ctypes.c_float),
         ("from_cache", ctypes.c_int),
         ("work_budget", ctypes.c_int),
+        ("deferred_chunks", ctypes.c_int),
+        ("reserved", ctypes.c_int),
     ]
 
     def as_dict(self):
@@ -177,6 +179,7 @@ def lib() -> ctypes.CDLL:
     L.dgt_validate.argtypes = [vp, vp, vp, vp, ctypes.c_int, ctypes.POINTER(Validation), vp]
     L.dgt_get_cell_order.argtypes = [vp, vp, vp]
     L.dgt_get_hilbert_order.argtypes = [vp, vp, vp, vp]
+    L.dgt_set_deferred_overlap.argtypes = [vp, ctypes.c_int]
     L.dgt_get_tuning.argtypes = [vp, P_D, P_I, P_I, P_I]
     L.dgt_autotune.argtypes = [vp, vp, vp, vp, ctypes.c_int, vp, ctypes.POINTER(TuneResult)]
     L.dgt_global_triangulation_noalloc.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,

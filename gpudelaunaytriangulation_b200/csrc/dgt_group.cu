@@ -355,8 +355,8 @@ __global__ void __launch_bounds__(BLOCK) k_build_grp(RingArgs A)
                 pid = A.worklist[t];
                 slot = A.slot_of[pid];
             } else {
-                slot = t;
-                pid = __ldg(&A.sidx[t]);
+                slot = A.item_base + t;
+                pid = __ldg(&A.sidx[slot]);
             }
         }
         const int si_ = (act && A.set_of) ? __ldg(&A.set_of[slot]) : 0;

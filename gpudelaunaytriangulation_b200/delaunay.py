@@ -347,6 +347,11 @@ class DelaunayGPU:
         warp-per-point kernel takes it over (0: every point goes to the warp kernel)."""
         _nat.check(self._L.dgt_set_work_budget(self._h, int(budget)), "dgt_set_work_budget")
 
+    def setDeferredOverlap(self, chunks: int):
+        """Global triangulations in `chunks` (1-8) pieces whose deferred points are rebuilt
+        while the next pieces build (same output; see dgt_set_deferred_overlap)."""
+        _nat.check(self._L.dgt_set_deferred_overlap(self._h, int(chunks)), "dgt_set_deferred_overlap")
+
     def tuning(self) -> dict:
         cs, sh, cap, blk = ctypes.c_double(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         _nat.check(self._L.dgt_get_tuning(self._h, ctypes.byref(cs), ctypes.byref(sh), ctypes.byref(cap),

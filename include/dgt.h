@@ -245,6 +245,13 @@ int dgt_set_kernel_shape(dgt_context *ctx, int shape);
  * of dense clusters, whose circles reach over large regions).  Default 1024; 0 sends every
  * point to the warp-per-point kernel.  Both kernels give the same rings. */
 int dgt_set_work_budget(dgt_context *ctx, int budget);
+/* Global triangulations in `chunks` (1-8) pieces of the cell order, the points each piece
+ * defers to the warp-per-point kernel rebuilt on a stream of their own while the next pieces
+ * build, so the slowest deferred points start early (clustered input; default 1: the whole
+ * build, then the deferred points).  The output is the same; while the call's stream is
+ * capturing a CUDA graph the build is not split.  dgt_autotune chooses it for clustered
+ * input. */
+int dgt_set_deferred_overlap(dgt_context *ctx, int chunks);
 /* Repair strategy (no reference counterpart): on (default), test-and-repair first flips the
  * illegal edges of valid fans (Lawson) and rebuilds only what flips cannot settle (inverted
  * or non-winding fans, inconsistent quadrilaterals); off, it rebuilds every flagged point
@@ -270,6 +277,8 @@ typedef struct dgt_tune_result {
     float default_ms;   /* build time with cell edge = mean spacing, shape 0 */
     int from_cache;
     int work_budget;    /* chosen work budget of the per-thread kernel (dgt_set_work_budget) */
+    int deferred_chunks; /* chosen overlap of the deferred points (dgt_set_deferred_overlap) */
+    int reserved;
 } dgt_tune_result;
 int dgt_autotune(dgt_context *ctx, const double *d_points, int *d_tri, int *d_neighnum, int stride, void *stream,
                  dgt_tune_result *out);

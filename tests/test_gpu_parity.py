@@ -430,6 +430,33 @@ def test_batched_clustered_sets_through_warp_kernel_match_oracle():
     b.close()
 
 
+def test_deferred_overlap_same_rings():
+    # the global build in 1, 2, 3 or 8 pieces, each piece's deferred points rebuilt on a stream
+    # of their own while the next pieces build: the same rings as the restated reference, with
+    # many points deferred (clustered input, fine cells, small work budget)
+    pts, L = W.gaussian_mixture(65536, components=64, sigma=2.0, L=256.0, seed=9)
+    n = len(pts)
+    ref = O.restated_global(pts, L, L, 1.0, 32)
+    P = torch.from_numpy(pts).cuda()
+    for chunks in (1, 2, 3, 8):
+        d = _dg()(n, 32, 0.25 * L / np.sqrt(n), (L, L))
+        d.setWorkBudget(64)
+        d.setDeferredOverlap(chunks)
+        tri = torch.zeros(32 * n, dtype=torch.int32, device="cuda")
+        nn = torch.zeros(n, dtype=torch.int32, device="cuda")
+        for _ in range(2):
+            d.globalDelaunayTriangulation(P, tri, nn)
+        st = d.stats()
+        assert st["error_flags"] == 0 and st["exact_points"] > 1000, (chunks, st)
+        t, k = host(tri, nn)
+        assert np.array_equal(k, ref.nn), chunks
+        assert np.array_equal(O.canonical(t, k), O.canonical(ref.tri, ref.nn)), chunks
+        for bad in (0, 9):
+            with pytest.raises(N.DgtError):
+                d.setDeferredOverlap(bad)
+        d.close()
+
+
 def test_million_points_properties():
     n = 1_000_000
     L = 1000.0
