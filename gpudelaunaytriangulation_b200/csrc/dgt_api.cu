@@ -103,13 +103,12 @@ struct dgt_context {
     int graph_flip_rounds = ASYNC_FLIP_ROUNDS;   // flip rounds of unsynchronised calls
     bool binned = false;   // the cell lists hold a binning of the current grid
     int flip_cap = 0;
-    // global builds in this many chunks of cell-order slots, each chunk's deferred points
-    // rebuilt on a stream of their own while the next chunks build (1: the whole build, then
-    // the deferred points)
+    // global builds in this many pieces of the cell order, each on a stream of its own with
+    // the points it defers (1: the whole build, then the deferred points)
     int defer_chunks = 1;
     cudaStream_t aux[MAX_DEFER_CHUNKS] = {};
-    cudaEvent_t chunk_ev[MAX_DEFER_CHUNKS] = {}, aux_ev[MAX_DEFER_CHUNKS] = {};
-    DevBuf dsnap;   // defer_count after each chunk
+    cudaEvent_t fork_ev = nullptr, aux_ev[MAX_DEFER_CHUNKS] = {};
+    DevBuf dcount;   // deferred count of each piece
 };
 
 namespace {
@@ -455,44 +454,41 @@ cudaError_t run_build(dgt_context *c, const RingArgs &a, cudaStream_t s)
                         a.repair ? 0 : c->shape, s);
 }
 
-// A global build in c->defer_chunks chunks of cell-order slots.  After each chunk a snapshot
-// of the deferred count is taken in stream order; the warp kernel for that chunk's deferred
-// points ([previous snapshot, this one) of the list) runs on a stream of its own, so it
-// overlaps the chunks that follow and the deferred points of different chunks overlap each
-// other (their run time is set by their slowest points, not by throughput).  No kernel waits
-// on another: the snapshot and the events order everything.  The call's stream waits for
-// every chunk's deferred points before it goes on.
+// A global build in c->defer_chunks pieces of the cell order, each on a stream of its own
+// and followed there by the warp kernel for the points it deferred.  Each piece appends to
+// its own segment of the deferred list (its own slots' range, so it cannot overflow) with its
+// own counter, so its warp kernel reads an exact count in stream order while the other pieces
+// still build.  The pieces overlap one another (no drain between them), and the slowest
+// deferred points start as soon as their piece is done.  Nothing spins: events fork the
+// pieces from the call's stream and join them back into it.
 cudaError_t run_build_chunked(dgt_context *c, const RingArgs &a, cudaStream_t s)
 {
     const int K = c->defer_chunks;
-    cudaError_t e = c->dsnap.ensure(sizeof(int) * MAX_DEFER_CHUNKS);
+    cudaError_t e = c->dcount.ensure(sizeof(int) * MAX_DEFER_CHUNKS);
     if (e != cudaSuccess) return e;
+    if (!c->fork_ev && (e = cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming)) != cudaSuccess) return e;
     for (int k = 0; k < K; ++k) {
         if (!c->aux[k] && (e = cudaStreamCreateWithFlags(&c->aux[k], cudaStreamNonBlocking)) != cudaSuccess) return e;
-        if (!c->chunk_ev[k] && (e = cudaEventCreateWithFlags(&c->chunk_ev[k], cudaEventDisableTiming)) != cudaSuccess)
-            return e;
         if (!c->aux_ev[k] && (e = cudaEventCreateWithFlags(&c->aux_ev[k], cudaEventDisableTiming)) != cudaSuccess)
             return e;
     }
-    int *snap = c->dsnap.as<int>();
+    int *cnt = c->dcount.as<int>();
+    if ((e = cudaMemsetAsync(cnt, 0, sizeof(int) * MAX_DEFER_CHUNKS, s)) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(c->fork_ev, s)) != cudaSuccess) return e;
     const int per = (c->n + K - 1) / K;
     int used = 0;
     for (int k = 0; k < K; ++k) {
-        const int lo = k * per, cnt = std::min(per, c->n - lo);
-        if (cnt <= 0) break;
+        const int lo = k * per, items = std::min(per, c->n - lo);
+        if (items <= 0) break;
+        if ((e = cudaStreamWaitEvent(c->aux[k], c->fork_ev, 0)) != cudaSuccess) return e;
         RingArgs ak = a;
         ak.item_base = lo;
-        ak.n_items = cnt;
-        if ((e = run_build(c, ak, s)) != cudaSuccess) return e;
-        if ((e = launch_snapshot(a.defer_count, snap + k, s)) != cudaSuccess) return e;
-        if ((e = cudaEventRecord(c->chunk_ev[k], s)) != cudaSuccess) return e;
-        if ((e = cudaStreamWaitEvent(c->aux[k], c->chunk_ev[k], 0)) != cudaSuccess) return e;
-        RingArgs dk = a;
-        dk.defer_from = k ? snap + k - 1 : nullptr;
-        dk.defer_to = snap + k;
-        if ((e = run_deferred(c, dk, c->aux[k])) != cudaSuccess) return e;
+        ak.n_items = items;
+        ak.defer_list = a.defer_list + lo;
+        ak.defer_count = cnt + k;
+        if ((e = run_build(c, ak, c->aux[k])) != cudaSuccess) return e;
+        if ((e = run_deferred(c, ak, c->aux[k])) != cudaSuccess) return e;
         if ((e = cudaEventRecord(c->aux_ev[k], c->aux[k])) != cudaSuccess) return e;
-        c->launches += 1;
         used = k + 1;
     }
     for (int k = 0; k < used; ++k)
@@ -670,13 +666,13 @@ void dgt_destroy(dgt_context *c)
     DevBuf *bufs[] = { &c->d_sets, &c->d_set_of, &c->ccount, &c->cstart, &c->cell_of, &c->rank, &c->sidx,
                        &c->slot_of, &c->spos, &c->bsum, &c->mark, &c->list0, &c->list1, &c->defer_list,
                        &c->st, &c->ctl, &c->bcount, &c->claim, &c->flip0, &c->flip1, &c->quad, &c->vcount,
-                       &c->hsets, &c->hcount, &c->hstart, &c->hsum, &c->hbucket, &c->hrank, &c->dsnap };
+                       &c->hsets, &c->hcount, &c->hstart, &c->hsum, &c->hbucket, &c->hrank, &c->dcount };
     for (DevBuf *b : bufs) b->release();
     for (int k = 0; k < MAX_DEFER_CHUNKS; ++k) {
         if (c->aux[k]) cudaStreamDestroy(c->aux[k]);
-        if (c->chunk_ev[k]) cudaEventDestroy(c->chunk_ev[k]);
         if (c->aux_ev[k]) cudaEventDestroy(c->aux_ev[k]);
     }
+    if (c->fork_ev) cudaEventDestroy(c->fork_ev);
     if (c->h_st) cudaFreeHost(c->h_st);
     for (int p = 0; p < DGT_NUM_PHASES; ++p)
         for (int k = 0; k < 2; ++k)
@@ -1430,10 +1426,9 @@ int dgt_autotune(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, 
         c->work_budget = best_budget;
     }
     // clustered inputs: the build in 2-4 pieces, the deferred points of each overlapping the
-    // pieces that follow (the deferred phase is set by its slowest points, which then start
-    // before the per-thread kernel has finished; 1M-point mixture: 8.25 ms in one piece,
-    // 7.16 / 7.86 / 9.88 ms in 2 / 4 / 8, every piece boundary draining the per-thread
-    // kernel's last wave)
+    // rest (the deferred phase is set by its slowest points, which then start before the
+    // per-thread kernel has finished; 1M-point mixture: 8.2-8.4 ms in one piece, 7.2-8.1 ms
+    // in 2-8, varying with where the slowest points fall)
     int best_chunks = 1;
     for (int k = 2; k <= 4 && contrast == 2 && rr == DGT_OK; ++k) {
         float ms = 0;

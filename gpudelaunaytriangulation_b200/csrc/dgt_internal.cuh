@@ -227,10 +227,6 @@ struct RingArgs {
     // scans longer than work_budget (cells + candidates)
     int *defer_list;
     int *defer_count;
-    // the entries [*defer_from, *defer_to) of defer_list are the warp kernel's (null: from 0 /
-    // to *defer_count): a global build in chunks hands each chunk's deferred points on while
-    // the next chunk builds
-    const int *defer_from, *defer_to;
     int item_base;     // without a work list: item t is slot item_base + t
     int work_budget;
     int warp_items;    // work lists of at most this many items are rebuilt by the warp kernel alone
@@ -337,8 +333,6 @@ cudaError_t launch_build(const RingArgs &a, int mode, int sms, int shape, cudaSt
 // the one-ring kernel with `lanes` (4 or 8) lanes per point (dgt_group.cu)
 cudaError_t launch_build_group(const RingArgs &a, int mode, int sms, int lanes, cudaStream_t s);
 cudaError_t launch_deferred(const RingArgs &a, int sms, cudaStream_t s);
-// *dst = *src on the device, in stream order (a snapshot of a counter)
-cudaError_t launch_snapshot(const int *src, int *dst, cudaStream_t s);
 // cells + candidates one point may scan in the per-thread kernel before the warp-per-point
 // kernel takes it over (clustered 1M-point mixture: 13.4 ms build at 1024 against 19.2 ms at
 // 4096; uniform points stay far below it)

@@ -401,14 +401,13 @@ __global__ void __launch_bounds__(WARP_KERNEL_WARPS * 32, 2) k_build_warp(RingAr
     // a short work list is rebuilt here directly (a warp per point has a far shorter latency
     // than one thread per point, and few points cannot hide it); otherwise the deferred points
     const bool direct = A.worklist && item_count(A) <= A.warp_items;
-    const int from = direct || !A.defer_from ? 0 : max(*A.defer_from, 0);
-    const int n = direct ? item_count(A) : min(A.defer_to ? *A.defer_to : *A.defer_count, A.npoints);
+    const int n = direct ? item_count(A) : min(*A.defer_count, A.npoints);
     const int *list = direct ? A.worklist : A.defer_list;
     if (direct && A.repair && blockIdx.x == 0 && threadIdx.x == 0 && n > 0) {
         atomicAdd(&A.st->repaired, (unsigned long long)n);
         atomicMax(&A.st->rounds, A.round + 1);
     }
-    for (int item = from + blockIdx.x * WARP_KERNEL_WARPS + wib; item < n; item += gridDim.x * WARP_KERNEL_WARPS) {
+    for (int item = blockIdx.x * WARP_KERNEL_WARPS + wib; item < n; item += gridDim.x * WARP_KERNEL_WARPS) {
         const int e = list[item];
         const int pid = e < 0 ? ~e : e;
         heavy += e < 0;
@@ -675,14 +674,6 @@ cudaError_t launch_deferred(const RingArgs &a, int sms, cudaStream_t s)
 {
     if (a.general) k_build_warp<true><<<max(sms, 1) * 2, WARP_KERNEL_WARPS * 32, 0, s>>>(a);
     else k_build_warp<false><<<max(sms, 1) * 2, WARP_KERNEL_WARPS * 32, 0, s>>>(a);
-    return cudaGetLastError();
-}
-
-__global__ void k_snapshot(const int *src, int *dst) { *dst = *src; }
-
-cudaError_t launch_snapshot(const int *src, int *dst, cudaStream_t s)
-{
-    k_snapshot<<<1, 1, 0, s>>>(src, dst);
     return cudaGetLastError();
 }
 
