@@ -52,7 +52,7 @@ BUILD_BYTES_PER_POINT = 16 + 4 + 4 + 24 + 4
 # dram__bytes_write.sum of one launch / points) on a 1,048,576-point capture of the same
 # kernel (the --profile build case below); traffic scales with the number of points at fixed
 # density, so the 4M launch is reported as this figure times its points.
-BUILD_DRAM_BYTES_PER_POINT_NCU = 87.5
+BUILD_DRAM_BYTES_PER_POINT_NCU = 87.3
 FALLBACK_HBM_GBS = 6650.0
 
 
