@@ -35,6 +35,7 @@ EXPORTED = [
     "dgt_get_tuning", "dgt_autotune", "dgt_set_work_budget", "dgt_set_flip_repair",
     "dgt_validate", "dgt_get_cell_order", "dgt_set_box_general", "dgt_get_box", "dgt_create_batch_general",
     "dgt_set_graph_flip_rounds", "dgt_get_hilbert_order", "dgt_set_deferred_overlap",
+    "dgt_hilbert_sort_points",
 ]
 STEP_AUTO = 0xFFFFFFFFFFFFFFFF
 NOALLOC_MAX_POINTS = 65536
@@ -179,6 +180,7 @@ def lib() -> ctypes.CDLL:
     L.dgt_validate.argtypes = [vp, vp, vp, vp, ctypes.c_int, ctypes.POINTER(Validation), vp]
     L.dgt_get_cell_order.argtypes = [vp, vp, vp]
     L.dgt_get_hilbert_order.argtypes = [vp, vp, vp, vp]
+    L.dgt_hilbert_sort_points.argtypes = [vp, vp, vp, vp]
     L.dgt_set_deferred_overlap.argtypes = [vp, ctypes.c_int]
     L.dgt_get_tuning.argtypes = [vp, P_D, P_I, P_I, P_I]
     L.dgt_autotune.argtypes = [vp, vp, vp, vp, ctypes.c_int, vp, ctypes.POINTER(TuneResult)]

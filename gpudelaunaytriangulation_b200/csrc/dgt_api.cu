@@ -88,7 +88,7 @@ struct dgt_context {
     int total_cells = 0;
     int total_blocks = 0;
     DevBuf d_sets, d_set_of, ccount, cstart, cell_of, rank, sidx, slot_of, spos, bsum, mark, list0, list1,
-        defer_list, st, ctl, bcount, claim, flip0, flip1, quad, vcount, hsets, hcount, hstart, hsum, hbucket, hrank;
+        defer_list, st, ctl, bcount, claim, flip0, flip1, quad, vcount, hsets, hcount, hstart, hsum, hbucket, hrank, horder, hperm;
     DevStatus *h_st = nullptr;
     cudaStream_t last_stream = nullptr;
     bool stats_valid = false;
@@ -668,7 +668,7 @@ void dgt_destroy(dgt_context *c)
     DevBuf *bufs[] = { &c->d_sets, &c->d_set_of, &c->ccount, &c->cstart, &c->cell_of, &c->rank, &c->sidx,
                        &c->slot_of, &c->spos, &c->bsum, &c->mark, &c->list0, &c->list1, &c->defer_list,
                        &c->st, &c->ctl, &c->bcount, &c->claim, &c->flip0, &c->flip1, &c->quad, &c->vcount,
-                       &c->hsets, &c->hcount, &c->hstart, &c->hsum, &c->hbucket, &c->hrank, &c->dcount };
+                       &c->hsets, &c->hcount, &c->hstart, &c->hsum, &c->hbucket, &c->hrank, &c->dcount, &c->horder, &c->hperm };
     for (DevBuf *b : bufs) b->release();
     for (int k = 0; k < MAX_DEFER_CHUNKS; ++k) {
         if (c->aux[k]) cudaStreamDestroy(c->aux[k]);
@@ -1223,6 +1223,25 @@ int dgt_get_hilbert_order(dgt_context *c, const double *d_points, int *d_order, 
     DGT_TRY(launch_hilbert_order(a, st));
     // the host copy of the descriptors must outlive the transfer
     DGT_TRY(cudaStreamSynchronize(st));
+    return DGT_OK;
+}
+
+int dgt_hilbert_sort_points(dgt_context *c, double *d_points, int *d_order, void *stream)
+{
+    if (!c) return DGT_ERR_INVALID_ARGUMENT;
+    if (c->n == 0) return DGT_OK;
+    if (!d_points) return DGT_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = (cudaStream_t)stream;
+    int *order = d_order;
+    if (!order) {
+        DGT_TRY(c->horder.ensure(sizeof(int) * (size_t)c->n));
+        order = c->horder.as<int>();
+    }
+    int r = dgt_get_hilbert_order(c, d_points, order, stream);
+    if (r != DGT_OK) return r;
+    DGT_TRY(c->hperm.ensure(sizeof(double2) * (size_t)c->n));
+    DGT_TRY(launch_gather_points(reinterpret_cast<const double2 *>(d_points), order, c->n, c->hperm.as<double2>(), s));
+    DGT_TRY(cudaMemcpyAsync(d_points, c->hperm.p, sizeof(double2) * (size_t)c->n, cudaMemcpyDeviceToDevice, s));
     return DGT_OK;
 }
 

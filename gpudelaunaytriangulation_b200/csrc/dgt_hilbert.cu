@@ -104,6 +104,18 @@ static int grid_for(long long items)
     return (int)(g < 1 ? 1 : (g > 65535 ? 65535 : g));
 }
 
+__global__ void __launch_bounds__(256) k_gather_points(const double2 *src, const int *order, int n, double2 *dst)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) dst[k] = src[order[k]];
+}
+
+cudaError_t launch_gather_points(const double2 *src, const int *order, int n, double2 *dst, cudaStream_t s)
+{
+    if (n <= 0) return cudaSuccess;
+    k_gather_points<<<grid_for(n), 256, 0, s>>>(src, order, n, dst);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_hilbert_order(const HilbertArgs &a, cudaStream_t s)
 {
     cudaError_t e = cudaMemsetAsync(a.hcount, 0, sizeof(int) * ((size_t)a.buckets + 1), s);

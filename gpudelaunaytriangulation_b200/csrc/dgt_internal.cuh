@@ -326,6 +326,8 @@ struct HilbertArgs {
     int *order;        // n: the result
 };
 cudaError_t launch_hilbert_order(const HilbertArgs &a, cudaStream_t s);
+// dst[k] = src[order[k]]
+cudaError_t launch_gather_points(const double2 *src, const int *order, int n, double2 *dst, cudaStream_t s);
 constexpr int KERNEL_SHAPES = 7;
 int kernel_shape_cap(int shape);
 int kernel_shape_block(int shape);

@@ -333,6 +333,17 @@ class DelaunayGPU:
                        "dgt_get_hilbert_order")
         return out
 
+    def hilbertSort(self, points: torch.Tensor, stream=None) -> torch.Tensor:
+        """Reorder `points` in place along hilbertOrder (the reference's hilbertSortArray,
+        triangulation.cpp:63-88); returns the order (point k is the old point order[k])."""
+        n = self.Ncells
+        _check_points(points, n)
+        out = torch.empty(n, dtype=torch.int32, device=points.device)
+        if n:
+            _nat.check(self._L.dgt_hilbert_sort_points(self._h, _ptr(points), _ptr(out), _stream_ptr(stream)),
+                       "dgt_hilbert_sort_points")
+        return out
+
     def setFlipRepair(self, on: bool):
         """Test-and-repair by Lawson flips first (default) or by rebuilding every flagged point."""
         _nat.check(self._L.dgt_set_flip_repair(self._h, int(bool(on))), "dgt_set_flip_repair")

@@ -201,6 +201,11 @@ int dgt_get_cell_order(dgt_context *ctx, int *d_order, void *stream);
  * int[n] on the device.  Allocates its scratch on first use (16 to 40 bytes per point, with
  * the grid) and synchronises `stream` before it returns. */
 int dgt_get_hilbert_order(dgt_context *ctx, const double *d_points, int *d_order, void *stream);
+/* The reference's hilbertSortArray (triangulation.cpp:63-88) on the device: reorders
+ * d_points in place along the order of dgt_get_hilbert_order (point k becomes the old point
+ * d_order[k]); d_order (int[n] on the device) receives that order, or may be null.  Existing
+ * triangulations refer to the old numbering: triangulate again after sorting. */
+int dgt_hilbert_sort_points(dgt_context *ctx, double *d_points, int *d_order, void *stream);
 
 /* 1: record CUDA events around each phase of every call (on the call's stream). */
 int dgt_set_timing(dgt_context *ctx, int on);

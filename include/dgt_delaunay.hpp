@@ -290,6 +290,14 @@ template <class BoxPtr> class DelaunayGPUT {
     void setWorkBudget(int budget) { check(dgt_set_work_budget(ctx(), budget), "setWorkBudget"); }
     void setGraphFlipRounds(int rounds) { check(dgt_set_graph_flip_rounds(ctx(), rounds), "setGraphFlipRounds"); }
     void setCheckMode(bool on) { check(dgt_set_check_mode(ctx(), on ? 1 : 0), "setCheckMode"); }
+    void setDeferredOverlap(int chunks) { check(dgt_set_deferred_overlap(ctx(), chunks), "setDeferredOverlap"); }
+    //! the reference driver's hilbertSortArray (triangulation.cpp:63-88) on the device: the
+    //! points reordered in place along a Hilbert curve over the box (triangulate again after)
+    template <class PointArray> void hilbertSortArray(PointArray &points)
+    {
+        check(dgt_hilbert_sort_points(ctx(), const_cast<double *>(pts(points)), nullptr, stream_),
+              "hilbertSortArray");
+    }
     //! the ring capacity as the library holds it (the same value as the MaxSize member)
     int getMaxSize() const
     {

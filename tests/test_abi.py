@@ -113,6 +113,7 @@ void use()
     int maxSize = delGPU.MaxSize;
     (void)maxSize;
     delGPU.prof.print();
+    delGPU.hilbertSortArray(gpuPts);   // the driver's hilbertSortArray pre-pass, on the device
     dgt::DelaunayGPU blank;
     blank.initialize(100, 16, 1.0, domain);
     blank.updateList(gpuPts);

@@ -96,3 +96,20 @@ def test_hilbert_renumbering_gives_same_rings_relabelled():
     assert np.median(span) < n / 50
     d.close()
     d2.close()
+
+
+def test_hilbert_sort_points_in_place():
+    # the reference driver's hilbertSortArray: points reordered in place along the curve
+    n = 20000
+    L = float(np.sqrt(n))
+    pts = W.uniform_points(n, L, 75)
+    d = _dg()(n, 16, 1.0, (L, L))
+    P = torch.from_numpy(pts.copy()).cuda()
+    order = d.hilbertSort(P).cpu().numpy().astype(np.int64)
+    ref = O.hilbert_order(pts, [n], [(L, L)])
+    assert np.array_equal(order, ref)
+    assert np.array_equal(P.cpu().numpy(), pts[ref])
+    # sorted again: already in curve order
+    again = d.hilbertSort(P).cpu().numpy()
+    assert np.array_equal(again, np.arange(n))
+    d.close()
