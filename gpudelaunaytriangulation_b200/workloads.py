@@ -82,6 +82,21 @@ def triangular_lattice(nx: int, ny: int, spacing: float = 1.0, jitter: float = 1
     return wrap(pts, Lx, Ly), Lx, Ly
 
 
+def square_lattice(n: int, phase: float = 0.25, seed: int = 4):
+    """The reference driver's squareLattice input (triangulation.cpp:39-61): a k x k square
+    lattice, k = ceil(sqrt(n)), of spacing sqrt(n) / k in the box of side sqrt(n), each site
+    drawn uniformly within +-phase spacings of its centre, sites taken column by column until
+    n are placed.  Returns (points, L)."""
+    L = math.sqrt(n)
+    k = int(math.ceil(math.sqrt(n)))
+    s = L / k
+    x, y = np.meshgrid(np.arange(k), np.arange(k), indexing="ij")   # x outer, y inner
+    centre = np.stack([x.ravel(), y.ravel()], axis=1)[:n].astype(np.float64) + 0.5
+    u = splitmix64_uniform(seed, 2 * n).reshape(-1, 2)
+    pts = s * (centre + (2.0 * u - 1.0) * phase)
+    return wrap(pts, L, L), L
+
+
 def gaussian_mixture(n: int, components: int = 64, sigma: float = 2.0, L: float | None = None, seed: int = 5):
     """n points from an equal-weight mixture of isotropic Gaussians (std sigma) whose centres are
     uniform in the periodic box of side L (default sqrt(n)), wrapped.  Returns (points, L)."""

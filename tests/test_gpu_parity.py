@@ -430,6 +430,27 @@ def test_batched_clustered_sets_through_warp_kernel_match_oracle():
     b.close()
 
 
+@pytest.mark.parametrize("n", [10000, 9000])
+def test_square_lattice_input_matches_reference(n):
+    # the reference driver's squareLattice input (jittered square lattice, near-cocircular
+    # squares; 9000 leaves the last column partly empty), build and one repair
+    pts, L = W.square_lattice(n, seed=11)
+    d, P, tri, nn = gpu_build(pts, L, L, 1.0, 16, True, check=True)
+    st = d.stats()
+    assert st["error_flags"] == 0 and st["mismatches"] == 0, st
+    t, k = host(tri, nn)
+    ref = O.restated_global(pts, L, L, 1.0, 32)
+    assert np.array_equal(k, ref.nn)
+    assert np.array_equal(O.canonical(t, k)[:, :16], O.canonical(ref.tri, ref.nn)[:, :16])
+    moved = W.displace(pts, 0.05, L, L, 12)
+    P.copy_(torch.from_numpy(moved))
+    d.testAndRepairDelaunayTriangulation(P, tri, nn)
+    t, k = host(tri, nn)
+    ref = O.restated_global(moved, L, L, 1.0, 32)
+    assert np.array_equal(k, ref.nn)
+    assert np.array_equal(O.canonical(t, k)[:, :16], O.canonical(ref.tri, ref.nn)[:, :16])
+
+
 def test_deferred_overlap_same_rings():
     # the global build in 1, 2, 3 or 8 pieces, each piece's deferred points rebuilt on a stream
     # of their own while the next pieces build: the same rings as the restated reference, with
