@@ -50,13 +50,16 @@ def test_too_few_points_report_an_error_and_leave_the_library_usable(n):
     assert d2.validate(Q, tri, nn)["valid"] == 1
 
 
-def test_batch_with_empty_and_tiny_sets():
+@pytest.mark.parametrize("pieces", [1, 8])
+def test_batch_with_empty_and_tiny_sets(pieces):
+    # pieces > 1: the global build split into pieces of the cell order that straddle the sets
     _, DelaunayBatch = _dg()
     sizes = np.array([0, 500, 0, 2000, 40], dtype=np.int64)
     boxes = np.stack([np.sqrt(np.maximum(sizes, 1).astype(np.float64))] * 2, axis=1)
     pts = np.concatenate([W.uniform_points(int(n), float(L), 300 + s)
                           for s, (n, L) in enumerate(zip(sizes, boxes[:, 0])) if n > 0])
     b = DelaunayBatch(sizes, boxes, 16, 1.0)
+    b.setDeferredOverlap(pieces)
     P = torch.from_numpy(pts).cuda()
     tri, nn = b.globalDelaunayTriangulation(P)
     t = tri.view(len(pts), -1).cpu().numpy()
@@ -72,6 +75,29 @@ def test_batch_with_empty_and_tiny_sets():
         assert np.array_equal(k[lo:hi], ref.nn), s
         assert np.array_equal(O.canonical(ts, k[lo:hi])[:, : t.shape[1]],
                               O.canonical(ref.tri, ref.nn)[:, : t.shape[1]]), s
+
+
+def test_few_points_in_many_pieces():
+    # 40 points in 8 pieces of 5 and 12 points in 8 pieces of 2 (the pieces past the last
+    # point are not launched): the same rings as in one piece, and the restated reference's
+    DelaunayGPU, _ = _dg()
+    for n, L, seed in ((40, 5.0, 3), (12, float(np.sqrt(12)), 93)):
+        pts = W.uniform_points(n, L, seed)
+        P = torch.from_numpy(pts).cuda()
+        out = []
+        for pieces in (1, 8):
+            d = DelaunayGPU(n, 16, 1.0, (L, L))
+            d.setDeferredOverlap(pieces)
+            tri, nn = d.globalDelaunayTriangulation(P)
+            out.append((tri.view(n, -1).cpu().numpy(), nn.cpu().numpy()))
+            d.close()
+        assert np.array_equal(out[0][1], out[1][1]) and np.array_equal(out[0][0], out[1][0]), n
+        assert (out[1][1] >= 3).all()
+        if n == 40:
+            ref = O.restated_global(pts, L, L, 1.0, 32)
+            t, k = out[1]
+            assert np.array_equal(k, ref.nn)
+            assert np.array_equal(O.canonical(t, k)[:, :16], O.canonical(ref.tri, ref.nn)[:, :16])
 
 
 def test_coordinates_on_the_box_edges():
