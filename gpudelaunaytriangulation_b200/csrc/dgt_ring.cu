@@ -283,29 +283,6 @@ __device__ int coop_run(B &b, const int lane)
         }
     };
 
-    // the cells [xa, xb] x [ya, yb] of strip q as 8 x 8-cell tiles (see strip_tile), one per
-    // lane; the live ones are scanned cell by cell
-    auto scan_tiles = [&](int xa, int xb, int ya, int yb, int q) {
-        const int ntile = (((xb - xa) >> BLOCK_SHIFT) + 1) * (((yb - ya) >> BLOCK_SHIFT) + 1);
-        for (int tb = 0; tb < ntile && status == R_OK; tb += 32) {
-            const int ti = tb + lane;
-            int ta = 0, tbx = -1, tc = 0, td = -1;
-            bool live = false;
-            if (ti < ntile) {
-                strip_tile(ti, q, xa, xb, ya, yb, BLOCK_SHIFT, ta, tbx, tc, td);
-                live = occupied(A.bcount, S.block_base, S.bxsize, BLOCK_SHIFT, S, b.ocx, b.ocy, ta, tbx, tc, td) &&
-                       b.rect_reached(ta, tbx, tc, td, fx, fy);
-            }
-            unsigned todo = __ballot_sync(0xffffffffu, live);
-            while (todo && status == R_OK) {
-                const int src = __ffs(todo) - 1;
-                todo &= todo - 1;
-                scan_cells(__shfl_sync(0xffffffffu, ta, src), __shfl_sync(0xffffffffu, tbx, src),
-                           __shfl_sync(0xffffffffu, tc, src), __shfl_sync(0xffffffffu, td, src), true);
-            }
-        }
-    };
-
     for (int phase = 0; status == R_OK && phase < max_phase; ++phase) {
         int nx0 = x0, nx1 = x1, ny0 = y0, ny1 = y1;
         if (phase >= 1) {
@@ -341,36 +318,85 @@ __device__ int coop_run(B &b, const int lane)
         for (int q = 0; q < 4 && status == R_OK; ++q) {
             const int sw = sxb[q] - sxa[q] + 1, sh = syb[q] - sya[q] + 1;
             if (sw <= 0 || sh <= 0) continue;
-            if (phase < 2 || sw * sh <= 512) {
-                scan_cells(sxa[q], sxb[q], sya[q], syb[q], phase >= 2);
-                continue;
-            }
-            // a large strip: tiles first, one per lane, nearest first; a tile is opened only
-            // when an occupancy block it touches holds points and its rectangle meets a current
-            // circle (empty space costs one test per tile, not per cell).  A strip of more than
-            // 64 tiles of 8 x 8 cells is cut into 64 x 64-cell tiles first, judged by the
-            // super-block occupancy, and only those are opened into 8 x 8-cell tiles.
-            if ((((sw - 1) >> BLOCK_SHIFT) + 1) * (((sh - 1) >> BLOCK_SHIFT) + 1) <= 64) {
-                scan_tiles(sxa[q], sxb[q], sya[q], syb[q], q);
-                continue;
-            }
-            const int ntile = (((sw - 1) >> SBLOCK_SHIFT) + 1) * (((sh - 1) >> SBLOCK_SHIFT) + 1);
-            for (int tb = 0; tb < ntile && status == R_OK; tb += 32) {
-                const int ti = tb + lane;
-                int ta = 0, tbx = -1, tc = 0, td = -1;
-                bool live = false;
-                if (ti < ntile) {
-                    strip_tile(ti, q, sxa[q], sxb[q], sya[q], syb[q], SBLOCK_SHIFT, ta, tbx, tc, td);
-                    live = occupied(A.bcount, S.sblock_base, S.sbxsize, SBLOCK_SHIFT, S, b.ocx, b.ocy, ta, tbx, tc, td) &&
-                           b.rect_reached(ta, tbx, tc, td, fx, fy);
+            // a small strip (and the first two phases): its cells directly.  A large strip:
+            // tiles first, one per lane, nearest first; a tile is opened only when an occupancy
+            // block it touches holds points and its rectangle meets a current circle (empty
+            // space costs one test per tile, not per cell).  A strip of more than 64 tiles of
+            // 8 x 8 cells is cut into 64 x 64-cell tiles first, judged by the super-block
+            // occupancy, and only those are opened into 8 x 8-cell tiles.  One loop with one
+            // call of scan_cells: the candidate code is large and shared by few warps, and a
+            // single copy of it stays in the instruction cache.
+            const bool direct = phase < 2 || sw * sh <= 512;
+            const bool super = !direct && (((sw - 1) >> BLOCK_SHIFT) + 1) * (((sh - 1) >> BLOCK_SHIFT) + 1) > 64;
+            bool cells = direct;   // the rectangle [ca, cb] x [cc, cd] is to be scanned
+            int ca = sxa[q], cb = sxb[q], cc = sya[q], cd = syb[q];
+            bool prune = phase >= 2;
+            // 8 x 8-cell tiles over [ra, rb] x [rc, rd]: batch t1 of n1, live ones in todo1
+            int ra = sxa[q], rb = sxb[q], rc = sya[q], rd = syb[q];
+            int t1 = 0, n1 = (direct || super) ? 0 : (((sw - 1) >> BLOCK_SHIFT) + 1) * (((sh - 1) >> BLOCK_SHIFT) + 1);
+            unsigned todo1 = 0;
+            int ta1 = 0, tb1 = -1, tc1 = 0, td1 = -1;
+            // 64 x 64-cell tiles over the strip
+            int t2 = 0, n2 = super ? (((sw - 1) >> SBLOCK_SHIFT) + 1) * (((sh - 1) >> SBLOCK_SHIFT) + 1) : 0;
+            unsigned todo2 = 0;
+            int ta2 = 0, tb2 = -1, tc2 = 0, td2 = -1;
+            while (status == R_OK) {
+                if (cells) {
+                    cells = false;
+                    scan_cells(ca, cb, cc, cd, prune);
+                    continue;
                 }
-                unsigned todo = __ballot_sync(0xffffffffu, live);
-                while (todo && status == R_OK) {
-                    const int src = __ffs(todo) - 1;
-                    todo &= todo - 1;
-                    scan_tiles(__shfl_sync(0xffffffffu, ta, src), __shfl_sync(0xffffffffu, tbx, src),
-                               __shfl_sync(0xffffffffu, tc, src), __shfl_sync(0xffffffffu, td, src), q);
+                if (todo1) {
+                    const int src = __ffs(todo1) - 1;
+                    todo1 &= todo1 - 1;
+                    ca = __shfl_sync(0xffffffffu, ta1, src);
+                    cb = __shfl_sync(0xffffffffu, tb1, src);
+                    cc = __shfl_sync(0xffffffffu, tc1, src);
+                    cd = __shfl_sync(0xffffffffu, td1, src);
+                    prune = true;
+                    cells = true;
+                    continue;
                 }
+                if (t1 < n1) {
+                    const int ti = t1 + lane;
+                    bool live = false;
+                    ta1 = 0, tb1 = -1, tc1 = 0, td1 = -1;
+                    if (ti < n1) {
+                        strip_tile(ti, q, ra, rb, rc, rd, BLOCK_SHIFT, ta1, tb1, tc1, td1);
+                        live = occupied(A.bcount, S.block_base, S.bxsize, BLOCK_SHIFT, S, b.ocx, b.ocy, ta1, tb1, tc1,
+                                        td1) &&
+                               b.rect_reached(ta1, tb1, tc1, td1, fx, fy);
+                    }
+                    todo1 = __ballot_sync(0xffffffffu, live);
+                    t1 += 32;
+                    continue;
+                }
+                if (todo2) {
+                    const int src = __ffs(todo2) - 1;
+                    todo2 &= todo2 - 1;
+                    ra = __shfl_sync(0xffffffffu, ta2, src);
+                    rb = __shfl_sync(0xffffffffu, tb2, src);
+                    rc = __shfl_sync(0xffffffffu, tc2, src);
+                    rd = __shfl_sync(0xffffffffu, td2, src);
+                    t1 = 0;
+                    n1 = (((rb - ra) >> BLOCK_SHIFT) + 1) * (((rd - rc) >> BLOCK_SHIFT) + 1);
+                    continue;
+                }
+                if (t2 < n2) {
+                    const int ti = t2 + lane;
+                    bool live = false;
+                    ta2 = 0, tb2 = -1, tc2 = 0, td2 = -1;
+                    if (ti < n2) {
+                        strip_tile(ti, q, sxa[q], sxb[q], sya[q], syb[q], SBLOCK_SHIFT, ta2, tb2, tc2, td2);
+                        live = occupied(A.bcount, S.sblock_base, S.sbxsize, SBLOCK_SHIFT, S, b.ocx, b.ocy, ta2, tb2,
+                                        tc2, td2) &&
+                               b.rect_reached(ta2, tb2, tc2, td2, fx, fy);
+                    }
+                    todo2 = __ballot_sync(0xffffffffu, live);
+                    t2 += 32;
+                    continue;
+                }
+                break;
             }
         }
         x0 = nx0;
