@@ -241,3 +241,28 @@ def test_kernel_box_is_the_oracle_reduction():
         d = DelaunayGPU(100, 16, 1.0, PeriodicBox.general(*box))
         assert d.kernelBox() == O.reduce_basis(box)
         d.close()
+
+
+@pytest.mark.parametrize("shape", [HEX, OBLIQUE], ids=["hex", "oblique"])
+def test_oblique_box_deferred_points_in_pieces(shape):
+    # work budget 16 sends most points to the warp-per-point kernel (its general-box tile
+    # walk), and the build runs in 1 or 5 overlapped pieces: the same rings as the default
+    # build, accepted by the exact verifier
+    DelaunayGPU, _ = _dgpu()
+    n = 20000
+    box = _box_of_area(n, shape)
+    pts = _oblique_points(n, box, 47)
+    _, _, _, _, t0, k0 = _build(pts, box)
+    P = torch.from_numpy(pts).cuda()
+    for pieces in (1, 5):
+        d = DelaunayGPU(n, 16, 1.0, box)
+        d.setWorkBudget(16)
+        d.setDeferredOverlap(pieces)
+        tri, nn = d.globalDelaunayTriangulation(P)
+        st = d.stats()
+        assert st["error_flags"] == 0 and st["exact_points"] > n // 4, (pieces, st)
+        t = tri.view(n, -1).cpu().numpy()
+        k = nn.cpu().numpy()
+        assert _same_rings(t0, k0, t, k), pieces
+        assert d.validate(P, tri, nn)["valid"] == 1
+        d.close()
