@@ -386,7 +386,8 @@ cudaError_t run_bin(dgt_context *c, const double *pts, cudaStream_t s)
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(c->bcount.p, 0, sizeof(int) * ((size_t)c->total_blocks + 1), s);
     if (e != cudaSuccess) return e;
-    c->launches += (c->n > 0 ? 2 : 0) + 3 + (c->deterministic && c->total_cells > 0 ? 1 : 0);
+    // count, super-block occupancy and scatter; three scan kernels; the in-cell order
+    c->launches += (c->n > 0 ? 3 : 0) + 3 + (c->deterministic && c->total_cells > 0 ? 1 : 0);
     e = launch_bin_st(bin_args(c, pts), c->st.as<DevStatus>(), s);
     if (e == cudaSuccess) c->binned = true;
     return e;
@@ -406,7 +407,7 @@ cudaError_t run_bin_refresh(dgt_context *c, const double *pts, cudaStream_t s)
     e = launch_clear_counts(c->ccount.as<int>(), c->total_cells + 1, c->bcount.as<int>(), c->total_blocks + 1,
                             a.cond, s);
     if (e != cudaSuccess) return e;
-    c->launches += (c->n > 0 ? 5 : 3) + 3 + (c->deterministic && c->total_cells > 0 ? 1 : 0);
+    c->launches += (c->n > 0 ? 6 : 3) + 3 + (c->deterministic && c->total_cells > 0 ? 1 : 0);
     return launch_bin_st(a, st, s);
 }
 
@@ -841,7 +842,7 @@ int repair_impl(dgt_context *c, const double *d_points, int *d_tri, int *d_nn, i
         DGT_TRY(launch_clear_counts(c->ccount.as<int>(), c->total_cells + 1, c->bcount.as<int>(), c->total_blocks + 1,
                                     a.cond, s));
         DGT_TRY(launch_bin_st(a, dst, s));
-        c->launches += 2 + (c->n > 0 ? 2 : 0) + 3 + (c->deterministic && c->total_cells > 0 ? 1 : 0);
+        c->launches += 2 + (c->n > 0 ? 3 : 0) + 3 + (c->deterministic && c->total_cells > 0 ? 1 : 0);
     }
     if (c->flip) {
         c->launches += 1;
